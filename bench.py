@@ -1,0 +1,341 @@
+"""Benchmark: BCn encode throughput on B200 (Mpixel/s).
+
+Workload (one "step"): the 2048x2048 RGBA8 texture-with-alpha workload
+encoded four ways -- BC7 (alpha_basic profile), BC3 and BC4 (R channel) of the
+colour+alpha image, and BC5 of a 2048x2048 normal map -- i.e. 4 x 4.19 Mpx of
+encoded texels per step. Seeded synthetic content (block_compression_b200.
+synthetic); no dataset is involved.
+
+value: encoded Mpixel/s over the whole job (all ranks), device-resident
+  inputs, CUDA-event timed per step with an L2 flush (a 256 MiB write)
+  before every step.
+e2e:   the same metric through the public host-buffer entry points
+  (bc_compress_rgba8 with pinned host buffers: H2D copy, kernel, D2H copy,
+  synchronize), as a reference user would call compress_rgba8.
+
+--impl reference times the reference algorithm on the host CPU (the C++
+restatement of the Rust encoder in oracle/, all host threads) on a bounded
+sample of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); each rank encodes its own copy of
+the workload (independent textures, no data exchange); max-over-ranks device
+time, weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = H = 2048
+METRIC = "BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
+WORKLOAD = "2048x2048 RGBA8 alpha texture: BC7 alpha_basic + BC3 + BC4(R); 2048x2048 normal map: BC5"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference(args, world, rank):
+    """Reference arm: the reference's encoder restated in C++ (oracle/), all
+    host threads, on a bounded sample of the workload."""
+    import numpy as np
+
+    import oracle
+    from block_compression_b200 import synthetic
+
+    if rank != 0:
+        return
+    img = synthetic.config2_image(seed=2, size=W)
+    nrm = synthetic.normal_map(seed=2, size=W)
+    threads = os.cpu_count()
+    a7 = [2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 12, 8, 8, 0, 2, 4]  # BC7Settings::alpha_basic()
+    # bounded sample: the full image for BC3/BC4/BC5 and a 256-row band for BC7
+    band = 256
+    crop = np.ascontiguousarray(img[:band])
+
+    def step():
+        t0 = time.perf_counter()
+        oracle.compress_rgba8(6, crop, W, band, settings=a7, threads=threads)
+        t7 = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.compress_rgba8(2, img, W, H, threads=threads)
+        oracle.compress_rgba8(3, img, W, H, threads=threads)
+        oracle.compress_rgba8(4, nrm, W, H, threads=threads)
+        t345 = time.perf_counter() - t0
+        # full-step time extrapolated from the BC7 band
+        return t7 * (H / band) + t345
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    times = [step() for _ in range(args.steps)]
+    t = sum(times) / len(times)
+    value = 4 * W * H / t / 1e6
+    sample = "BC7 on a %dx%d band (time scaled x%d), BC3/BC4/BC5 on the full images" % (W, band, H // band)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_bench(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import block_compression_b200 as bcn
+    from block_compression_b200 import synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    V = bcn.CompressionVariant
+    s7 = bcn.BC7Settings.alpha_basic()
+    jobs = [("bc7_alpha_basic", V.BC7(s7), "img"), ("bc3", V.BC3, "img"), ("bc4", V.BC4, "img"), ("bc5", V.BC5, "nrm")]
+    img_np = synthetic.config2_image(seed=2, size=W)
+    nrm_np = synthetic.normal_map(seed=2, size=W)
+    srcs = {"img": torch.from_numpy(img_np).to(dev), "nrm": torch.from_numpy(nrm_np).to(dev)}
+    outs = {name: torch.zeros(v.blocks_byte_size(W, H), dtype=torch.uint8, device=dev) for name, v, _ in jobs}
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    import ctypes
+    sp = ctypes.c_void_p(sptr)
+
+    def run_step(evs=None):
+        for i, (name, v, key) in enumerate(jobs):
+            if evs is not None:
+                evs[i][0].record(stream)
+            bcn.encode.compress_rgba8(v, srcs[key], outs[name], W, H, W * 4, stream=sp)
+            if evs is not None:
+                evs[i][1].record(stream)
+
+    for _ in range(max(3, args.warmup)):
+        flush.fill_(1)
+        run_step()
+    torch.cuda.synchronize()
+
+    step_ms, per_job = [], {name: [] for name, _, _ in jobs}
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)  # evict the inputs from L2 (126 MB) before each step
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in jobs]
+            run_step(evs)
+            torch.cuda.synchronize()
+            t = 0.0
+            for (name, _, _), (a, b) in zip(jobs, evs):
+                ms = a.elapsed_time(b)
+                per_job[name].append(ms)
+                t += ms
+            step_ms.append(t)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    total_ms = sum(step_ms)
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    px_per_step = 4 * W * H
+    value = world * px_per_step * args.steps / (total_ms / 1e3) / 1e6
+
+    # e2e through the host entry points with pinned host buffers
+    pin_img = torch.from_numpy(img_np).pin_memory()
+    pin_nrm = torch.from_numpy(nrm_np).pin_memory()
+    host_src = {"img": pin_img.numpy(), "nrm": pin_nrm.numpy()}
+    pin_out = {name: torch.zeros(v.blocks_byte_size(W, H), dtype=torch.uint8).pin_memory() for name, v, _ in jobs}
+    host_out = {k: t.numpy() for k, t in pin_out.items()}
+
+    def e2e_step():
+        for name, v, key in jobs:
+            bcn.encode.compress_rgba8(v, host_src[key], host_out[name], W, H, W * 4)
+
+    for _ in range(2):
+        e2e_step()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * px_per_step * args.steps / (e2e_ms / 1e3) / 1e6
+    h2d = 3 * img_np.nbytes + nrm_np.nbytes
+    d2h = sum(v.blocks_byte_size(W, H) for _, v, _ in jobs)
+
+    # correctness guard on the benchmarked output: a sample of blocks vs the oracle
+    import oracle
+    verified = None
+    if rank == 0:
+        rng = np.random.default_rng(0)
+        bw = W // 4
+        idx = rng.choice((W // 4) * (H // 4), 64, replace=False)
+        tiles = np.stack([img_np[(i // bw) * 4:(i // bw) * 4 + 4, (i % bw) * 4:(i % bw) * 4 + 4] for i in idx])
+        tile_img = np.ascontiguousarray(tiles.transpose(1, 0, 2, 3).reshape(4, 64 * 4, 4))
+        exp = oracle.compress_rgba8(6, tile_img, 256, 4, settings=s7.as_list()).reshape(64, 16)
+        got = outs["bc7_alpha_basic"].cpu().numpy().reshape(-1, 16)[idx]
+        verified = bool(np.array_equal(exp, got))
+
+    # CPU baseline (rank 0, N=1): bounded sample on all host threads
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count()
+        band = 128
+        crop = np.ascontiguousarray(img_np[:band])
+        t0 = time.perf_counter()
+        oracle.compress_rgba8(6, crop, W, band, settings=s7.as_list(), threads=threads)
+        t7 = (time.perf_counter() - t0) * (H / band)
+        t0 = time.perf_counter()
+        oracle.compress_rgba8(2, img_np, W, H, threads=threads)
+        oracle.compress_rgba8(3, img_np, W, H, threads=threads)
+        oracle.compress_rgba8(4, nrm_np, W, H, threads=threads)
+        t345 = time.perf_counter() - t0
+        cpu = {"value": px_per_step / (t7 + t345) / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
+               "sample": "BC7 on a %dx%d band scaled to the full image; BC3/BC4/BC5 full" % (W, band)}
+
+    peaks, src = _peaks()
+    bc7_ms = sum(per_job["bc7_alpha_basic"]) / len(per_job["bc7_alpha_basic"])
+    bc3_ms = sum(per_job["bc3"]) / len(per_job["bc3"])
+    if rank == 0:
+        per_variant = {name: W * H / (sum(ms) / len(ms) / 1e3) / 1e6 for name, ms in per_job.items()}
+        roof = {
+            "kernel": "bc7_encode_kernel", "bound": "issue", "unit": "Gblock/s",
+            "achieved": (W // 4) * (H // 4) / (bc7_ms / 1e3) / 1e9,
+            "peak": None, "frac": None, "traffic": None,
+            "note": "compute (FP32/INT issue) bound; see profiles/ for the issue-rate fraction",
+        }
+        bc3_bytes = W * H * 4 + (W // 4) * (H // 4) * 16
+        hbm = {"kernel": "bc15_encode_kernel<BC3>", "bound": "hbm", "unit": "GB/s",
+               "achieved": bc3_bytes / (bc3_ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"],
+               "frac": bc3_bytes / (bc3_ms / 1e3) / 1e9 / peaks["hbm_gbs"], "peak_source": src}
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "px_per_step": px_per_step, "l2": "flushed (256 MiB write) before each step",
+                       "bc7_settings": "alpha_basic"},
+            "e2e": {"value": e2e_value, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": len(jobs) * args.steps,
+            "per_variant_mpx_s": per_variant,
+            "roofline": roof, "roofline_hbm_path": hbm,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "verified_bc7_sample": verified,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    world, rank, local = _dist()
+    if args.impl == "reference":
+        cpu_reference(args, world, rank)
+    else:
+        gpu_bench(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,488 @@
+// BC1-BC5 encode and decode kernels for sm_100a.
+//
+// Bandwidth-bound paths: one thread owns one 4x4 block. A warp covers 32
+// neighbouring blocks of a block row, so each of the 4 source rows is read as
+// one contiguous 512-byte span of 128-bit loads, and the 8/16-byte outputs of
+// the warp land in one contiguous span as 64/128-bit stores. The per-block
+// arithmetic follows the reference encoder (src/encode/bc1_to_5.rs) operation
+// for operation so the output is bit-identical; see bc_common.cuh for the
+// float rules.
+#include <cuda_runtime.h>
+
+#include "bc_common.cuh"
+#include "bc_kernels.h"
+
+namespace bcn {
+
+// ---- BC1 colour (bc1_to_5.rs:157-429) ---------------------------------------
+
+struct Px16 {
+    float r[16], g[16], b[16], a[16];
+};
+
+BCN_DEV void dec_rgb565(float c[3], int p) {
+    int b5 = p & 31, g6 = (p >> 5) & 63, r5 = (p >> 11) & 31;
+    c[0] = (float)((r5 << 3) + (r5 >> 2));
+    c[1] = (float)((g6 << 2) + (g6 >> 4));
+    c[2] = (float)((b5 << 3) + (b5 >> 2));
+}
+
+BCN_DEV int enc_rgb565(float c0, float c1, float c2) {
+    int r = (int)c0, g = (int)c1, b = (int)c2;
+    int r5 = (r * 31 + 128 + ((r * 31) >> 8)) >> 8;
+    int g6 = (g * 63 + 128 + ((g * 63) >> 8)) >> 8;
+    int b5 = (b * 31 + 128 + ((b * 31) >> 8)) >> 8;
+    return (r5 << 11) + (g6 << 5) + b5;
+}
+
+// bc1_to_5.rs:280-321: 2-bit index per pixel by projection onto the
+// quantised endpoint direction.
+BCN_DEV uint32_t fast_quant(const Px16& px, int p0, int p1) {
+    float c0[3], c1[3], dir[3];
+    dec_rgb565(c0, p0);
+    dec_rgb565(c1, p1);
+    for (int p = 0; p < 3; p++) dir[p] = c1[p] - c0[p];
+    float sq_norm = 0.0f;
+    for (int p = 0; p < 3; p++) sq_norm += dir[p] * dir[p];
+    float rsq_norm = 1.0f / sq_norm;
+    for (int p = 0; p < 3; p++) dir[p] *= rsq_norm * 3.0f;
+    float bias = 0.5f;
+    for (int p = 0; p < 3; p++) bias -= c0[p] * dir[p];
+    uint32_t bits = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        float dot = 0.0f;
+        dot += px.r[k] * dir[0];
+        dot += px.g[k] * dir[1];
+        dot += px.b[k] * dir[2];
+        int q = clampi((int)(dot + bias), 0, 3);
+        bits += (uint32_t)q << (2 * k);
+    }
+    return bits;
+}
+
+// bc1_to_5.rs:323-374: least-squares endpoints for fixed indices.
+BCN_DEV void bc1_refine(const Px16& px, int pe[2], uint32_t bits, const float dc[3]) {
+    float c0[3], c1[3];
+    if ((bits ^ (bits * 4u)) < 4) {
+        for (int p = 0; p < 3; p++) c0[p] = c1[p] = dc[p];
+    } else {
+        float atb1[3] = {0.0f, 0.0f, 0.0f};
+        float sum_q = 0.0f, sum_qq = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            float q = (float)((bits >> (2 * k)) & 3);
+            float x = 3.0f - q;
+            sum_q += q;
+            sum_qq += q * q;
+            atb1[0] += x * px.r[k];
+            atb1[1] += x * px.g[k];
+            atb1[2] += x * px.b[k];
+        }
+        float sum[3], atb2[3];
+        for (int p = 0; p < 3; p++) {
+            sum[p] = dc[p] * 16.0f;
+            atb2[p] = 3.0f * sum[p] - atb1[p];
+        }
+        float cxx = 144.0f - 6.0f * sum_q + sum_qq;  // 16*9 - (2*3)*sum_q + sum_qq
+        float cyy = sum_qq;
+        float cxy = 3.0f * sum_q - sum_qq;
+        float scale = 3.0f * (1.0f / (cxx * cyy - cxy * cxy));
+        for (int p = 0; p < 3; p++) {
+            c0[p] = clampf_r((atb1[p] * cyy - atb2[p] * cxy) * scale, 0.0f, 255.0f);
+            c1[p] = clampf_r((atb2[p] * cxx - atb1[p] * cxy) * scale, 0.0f, 255.0f);
+        }
+    }
+    pe[0] = enc_rgb565(c0[0], c0[1], c0[2]);
+    pe[1] = enc_rgb565(c1[0], c1[1], c1[2]);
+}
+
+BCN_DEV uint32_t fix_qbits(uint32_t q) {
+    uint32_t q0 = q & 0x55555555u, q1 = q & 0xAAAAAAAAu;
+    return (q1 >> 1) + (q1 ^ (q0 << 1));
+}
+
+// bc1_to_5.rs:386-429
+BCN_DEV void bc1_core(const Px16& px, uint32_t& w0, uint32_t& w1) {
+    float dc[3];
+    {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += px.r[k];
+        dc[0] = acc / 16.0f;
+        acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += px.g[k];
+        dc[1] = acc / 16.0f;
+        acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += px.b[k];
+        dc[2] = acc / 16.0f;
+    }
+    float cv[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        float x0 = px.r[k] - dc[0], x1 = px.g[k] - dc[1], x2 = px.b[k] - dc[2];
+        cv[0] += x0 * x0;
+        cv[1] += x0 * x1;
+        cv[2] += x0 * x2;
+        cv[3] += x1 * x1;
+        cv[4] += x1 * x2;
+        cv[5] += x2 * x2;
+    }
+    const float eps = 1.1920929e-7f;  // f32::EPSILON
+    cv[0] += eps;
+    cv[3] += eps;
+    cv[5] += eps;
+    // compute_axis3, 4 power iterations, renormalised after the odd ones.
+    float a[3] = {1.0f, 1.0f, 1.0f}, ax[3];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        ax[0] = cv[0] * a[0] + cv[1] * a[1] + cv[2] * a[2];
+        ax[1] = cv[1] * a[0] + cv[3] * a[1] + cv[4] * a[2];
+        ax[2] = cv[2] * a[0] + cv[4] * a[1] + cv[5] * a[2];
+        a[0] = ax[0];
+        a[1] = ax[1];
+        a[2] = ax[2];
+        if (i % 2 == 1) {
+            float n = 0.0f;
+            n += ax[0] * ax[0];
+            n += ax[1] * ax[1];
+            n += ax[2] * ax[2];
+            float rn = 1.0f / sqrtf(n);
+            a[0] *= rn;
+            a[1] *= rn;
+            a[2] *= rn;
+        }
+    }
+    // pick_endpoints
+    float min_dot = 65536.0f, max_dot = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        float dot = 0.0f;
+        dot += (px.r[k] - dc[0]) * a[0];
+        dot += (px.g[k] - dc[1]) * a[1];
+        dot += (px.b[k] - dc[2]) * a[2];
+        min_dot = fminf(min_dot, dot);
+        max_dot = fmaxf(max_dot, dot);
+    }
+    if (max_dot - min_dot < 1.0f) {
+        min_dot -= 0.5f;
+        max_dot += 0.5f;
+    }
+    float norm_sq = 0.0f;
+    norm_sq += a[0] * a[0];
+    norm_sq += a[1] * a[1];
+    norm_sq += a[2] * a[2];
+    float rnorm_sq = 1.0f / norm_sq;
+    float c0[3], c1[3];
+    for (int p = 0; p < 3; p++) {
+        c0[p] = clampf_r(dc[p] + min_dot * rnorm_sq * a[p], 0.0f, 255.0f);
+        c1[p] = clampf_r(dc[p] + max_dot * rnorm_sq * a[p], 0.0f, 255.0f);
+    }
+    int p[2];
+    p[0] = enc_rgb565(c0[0], c0[1], c0[2]);
+    p[1] = enc_rgb565(c1[0], c1[1], c1[2]);
+    if (p[0] < p[1]) {
+        int t = p[0];
+        p[0] = p[1];
+        p[1] = t;
+    }
+    uint32_t q = fast_quant(px, p[0], p[1]);
+    // one refinement round (refine_iterations = 1)
+    bc1_refine(px, p, q, dc);
+    if (p[0] < p[1]) {
+        int t = p[0];
+        p[0] = p[1];
+        p[1] = t;
+    }
+    w0 = ((uint32_t)p[1] << 16) | (uint32_t)p[0];
+    w1 = fix_qbits(fast_quant(px, p[0], p[1]));
+}
+
+// bc1_to_5.rs:431-472: 8-level alpha / single channel block.
+BCN_DEV void bc3_alpha(const float* v, uint32_t& w0, uint32_t& w1) {
+    float e0 = 255.0f, e1 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        e0 = fminf(e0, v[k]);
+        e1 = fmaxf(e1, v[k]);
+    }
+    if (e0 == e1) e1 = e0 + 0.1f;
+    float scale = 7.0f / (e1 - e0);
+    uint32_t qb0 = 0, qb1 = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        float proj = (v[k] - e0) * scale + 0.5f;
+        int q = clampi((int)proj, 0, 7);
+        q = 7 - q;
+        if (q > 0) q += 1;
+        if (q == 8) q = 1;
+        if (k < 8) qb0 |= (uint32_t)q << (k * 3);
+        else qb1 |= (uint32_t)q << ((k - 8) * 3);
+    }
+    uint32_t a0 = min((uint32_t)e0, 255u), a1 = min((uint32_t)e1, 255u);
+    w0 = (a0 << 8) | a1 | (qb0 << 16);
+    w1 = (qb0 >> 16) | (qb1 << 8);
+}
+
+// ---- loads / stores -------------------------------------------------------
+
+// Loads the 4x4 RGBA8 block at (bx, by). ALIGNED: row base + 16*bx is
+// 16-byte aligned, so each row is one 128-bit load.
+template <bool ALIGNED>
+BCN_DEV void load_rgba8(const uint8_t* __restrict__ src, size_t stride, uint32_t bx, uint32_t by, Px16& px) {
+#pragma unroll
+    for (int y = 0; y < 4; y++) {
+        const uint8_t* row = src + (size_t)(by * 4 + y) * stride + (size_t)bx * 16;
+        uint32_t w[4];
+        if (ALIGNED) {
+            uint4 v = __ldg(reinterpret_cast<const uint4*>(row));
+            w[0] = v.x;
+            w[1] = v.y;
+            w[2] = v.z;
+            w[3] = v.w;
+        } else {
+            for (int x = 0; x < 4; x++)
+                w[x] = (uint32_t)row[4 * x] | ((uint32_t)row[4 * x + 1] << 8) | ((uint32_t)row[4 * x + 2] << 16) |
+                       ((uint32_t)row[4 * x + 3] << 24);
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            px.r[y * 4 + x] = (float)(w[x] & 0xFF);
+            px.g[y * 4 + x] = (float)((w[x] >> 8) & 0xFF);
+            px.b[y * 4 + x] = (float)((w[x] >> 16) & 0xFF);
+            px.a[y * 4 + x] = (float)(w[x] >> 24);
+        }
+    }
+}
+
+template <bool ALIGNED>
+BCN_DEV void store_block(uint8_t* dst, const uint32_t* w, int words) {
+    if (ALIGNED) {
+        if (words == 2) *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
+        else *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+        for (int i = 0; i < words; i++) reinterpret_cast<uint32_t*>(dst)[i] = w[i];
+    }
+}
+
+// ---- encode kernel -----------------------------------------------------------
+
+BCN_DEV void encode_bc15_block(int variant, const Px16& px, uint32_t w[4]) {
+    switch (variant) {
+        case BC_BC1:
+            bc1_core(px, w[0], w[1]);
+            break;
+        case BC_BC2: {
+            // bc1_to_5.rs:84-115
+            uint32_t a0 = 0, a1 = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                float alpha = px.a[k] / 255.0f;
+                uint32_t a4 = (uint32_t)(alpha * 15.0f);
+                if (k < 8) a0 |= a4 << (4 * k);
+                else a1 |= a4 << (4 * (k - 8));
+            }
+            w[0] = a0;
+            w[1] = a1;
+            bc1_core(px, w[2], w[3]);
+            break;
+        }
+        case BC_BC3:
+            bc3_alpha(px.a, w[0], w[1]);
+            bc1_core(px, w[2], w[3]);
+            break;
+        case BC_BC4:
+            bc3_alpha(px.r, w[0], w[1]);
+            break;
+        default:  // BC5
+            bc3_alpha(px.r, w[0], w[1]);
+            bc3_alpha(px.g, w[2], w[3]);
+            break;
+    }
+}
+
+template <int VARIANT, bool ALIGNED_SRC, bool ALIGNED_DST>
+__global__ void __launch_bounds__(128) bc15_encode_kernel(const uint8_t* __restrict__ src, size_t stride,
+                                                           uint32_t bw, uint32_t bh, uint8_t* __restrict__ dst) {
+    uint32_t n = bw * bh;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t by = i / bw, bx = i - by * bw;
+        Px16 px;
+        load_rgba8<ALIGNED_SRC>(src, stride, bx, by, px);
+        uint32_t w[4];
+        encode_bc15_block(VARIANT, px, w);
+        constexpr int words = (VARIANT == BC_BC1 || VARIANT == BC_BC4) ? 2 : 4;
+        store_block<ALIGNED_DST>(dst + (size_t)i * (words * 4), w, words);
+    }
+}
+
+// ---- BC1-BC5 decode (src/decode/block.rs:124-258, src/decode.rs:60-148) ------
+
+BCN_DEV void decode_color(uint32_t c01, uint32_t idx, bool opaque, uint32_t out[16]) {
+    uint32_t c0 = c01 & 0xFFFF, c1 = c01 >> 16;
+    uint32_t r0 = (c0 >> 11) & 0x1F, g0 = (c0 >> 5) & 0x3F, b0 = c0 & 0x1F;
+    uint32_t r1 = (c1 >> 11) & 0x1F, g1 = (c1 >> 5) & 0x3F, b1 = c1 & 0x1F;
+    uint32_t ref[4];
+    ref[0] = 0xFF000000u | (((b0 * 527 + 23) >> 6) << 16) | (((g0 * 259 + 33) >> 6) << 8) | ((r0 * 527 + 23) >> 6);
+    ref[1] = 0xFF000000u | (((b1 * 527 + 23) >> 6) << 16) | (((g1 * 259 + 33) >> 6) << 8) | ((r1 * 527 + 23) >> 6);
+    if (c0 > c1 || opaque) {
+        ref[2] = 0xFF000000u | ((((2 * b0 + b1) * 351 + 61) >> 7) << 16) | ((((2 * g0 + g1) * 2763 + 1039) >> 11) << 8) |
+                 (((2 * r0 + r1) * 351 + 61) >> 7);
+        ref[3] = 0xFF000000u | ((((b0 + 2 * b1) * 351 + 61) >> 7) << 16) | ((((g0 + 2 * g1) * 2763 + 1039) >> 11) << 8) |
+                 (((r0 + 2 * r1) * 351 + 61) >> 7);
+    } else {
+        ref[2] = 0xFF000000u | ((((b0 + b1) * 1053 + 125) >> 8) << 16) | ((((g0 + g1) * 4145 + 1019) >> 11) << 8) |
+                 (((r0 + r1) * 1053 + 125) >> 8);
+        ref[3] = 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) out[k] = ref[(idx >> (2 * k)) & 3];
+}
+
+BCN_DEV void decode_smooth(uint32_t lo, uint32_t hi, uint8_t out[16]) {
+    uint32_t a[8];
+    a[0] = lo & 0xFF;
+    a[1] = (lo >> 8) & 0xFF;
+    if (a[0] > a[1]) {
+        a[2] = (6 * a[0] + a[1]) / 7;
+        a[3] = (5 * a[0] + 2 * a[1]) / 7;
+        a[4] = (4 * a[0] + 3 * a[1]) / 7;
+        a[5] = (3 * a[0] + 4 * a[1]) / 7;
+        a[6] = (2 * a[0] + 5 * a[1]) / 7;
+        a[7] = (a[0] + 6 * a[1]) / 7;
+    } else {
+        a[2] = (4 * a[0] + a[1]) / 5;
+        a[3] = (3 * a[0] + 2 * a[1]) / 5;
+        a[4] = (2 * a[0] + 3 * a[1]) / 5;
+        a[5] = (a[0] + 4 * a[1]) / 5;
+        a[6] = 0;
+        a[7] = 255;
+    }
+    uint64_t idx = ((uint64_t)hi << 16) | (lo >> 16);
+#pragma unroll
+    for (int k = 0; k < 16; k++) out[k] = (uint8_t)a[(idx >> (3 * k)) & 7];
+}
+
+// Decodes one BC1-BC5 block to 16 RGBA8 pixels, with the reference's RGBA8
+// conventions (BC4 -> (R,0,0,0), BC5 -> (R,G,0,0)).
+BCN_DEV void decode_bc15_rgba8(int variant, const uint32_t* w, uint32_t out[16]) {
+    if (variant == BC_BC1) {
+        decode_color(w[0], w[1], false, out);
+    } else if (variant == BC_BC2) {
+        decode_color(w[2], w[3], true, out);
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            uint32_t a = ((k < 8 ? w[0] : w[1]) >> (4 * (k & 7))) & 15;
+            out[k] = (out[k] & 0x00FFFFFFu) | ((a * 17) << 24);
+        }
+    } else if (variant == BC_BC3) {
+        decode_color(w[2], w[3], true, out);
+        uint8_t a[16];
+        decode_smooth(w[0], w[1], a);
+#pragma unroll
+        for (int k = 0; k < 16; k++) out[k] = (out[k] & 0x00FFFFFFu) | ((uint32_t)a[k] << 24);
+    } else if (variant == BC_BC4) {
+        uint8_t r[16];
+        decode_smooth(w[0], w[1], r);
+#pragma unroll
+        for (int k = 0; k < 16; k++) out[k] = r[k];
+    } else {
+        uint8_t r[16], g[16];
+        decode_smooth(w[0], w[1], r);
+        decode_smooth(w[2], w[3], g);
+#pragma unroll
+        for (int k = 0; k < 16; k++) out[k] = (uint32_t)r[k] | ((uint32_t)g[k] << 8);
+    }
+}
+
+template <int VARIANT>
+__global__ void __launch_bounds__(128) bc15_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
+                                                           uint8_t* __restrict__ out, size_t pitch, bool aligned) {
+    constexpr int words = (VARIANT == BC_BC1 || VARIANT == BC_BC4) ? 2 : 4;
+    uint32_t n = bw * bh;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t by = i / bw, bx = i - by * bw;
+        uint32_t w[4] = {0, 0, 0, 0};
+        const uint8_t* b = blocks + (size_t)i * words * 4;
+        if (aligned) {
+            if (words == 2) {
+                uint2 v = __ldg(reinterpret_cast<const uint2*>(b));
+                w[0] = v.x;
+                w[1] = v.y;
+            } else {
+                uint4 v = __ldg(reinterpret_cast<const uint4*>(b));
+                w[0] = v.x;
+                w[1] = v.y;
+                w[2] = v.z;
+                w[3] = v.w;
+            }
+        } else {
+            for (int j = 0; j < words * 4; j++) w[j >> 2] |= (uint32_t)b[j] << (8 * (j & 3));
+        }
+        uint32_t px[16];
+        decode_bc15_rgba8(VARIANT, w, px);
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            uint8_t* row = out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
+            if (aligned) {
+                *reinterpret_cast<uint4*>(row) = make_uint4(px[y * 4], px[y * 4 + 1], px[y * 4 + 2], px[y * 4 + 3]);
+            } else {
+                for (int x = 0; x < 4; x++)
+                    for (int c = 0; c < 4; c++) row[4 * x + c] = (uint8_t)(px[y * 4 + x] >> (8 * c));
+            }
+        }
+    }
+}
+
+// ---- launchers ------------------------------------------------------------------
+
+static int grid_for(uint32_t n, int threads) {
+    // Enough CTAs to fill the machine several times over; the kernels loop
+    // grid-stride over any remainder.
+    uint32_t g = (n + threads - 1) / threads;
+    return (int)(g > 148u * 64u ? 148u * 64u : (g == 0 ? 1 : g));
+}
+
+template <int V>
+static void launch_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst, bool asrc,
+                          bool adst, cudaStream_t s) {
+    int g = grid_for(bw * bh, 128);
+    if (asrc && adst) bc15_encode_kernel<V, true, true><<<g, 128, 0, s>>>(src, stride, bw, bh, dst);
+    else if (asrc) bc15_encode_kernel<V, true, false><<<g, 128, 0, s>>>(src, stride, bw, bh, dst);
+    else if (adst) bc15_encode_kernel<V, false, true><<<g, 128, 0, s>>>(src, stride, bw, bh, dst);
+    else bc15_encode_kernel<V, false, false><<<g, 128, 0, s>>>(src, stride, bw, bh, dst);
+}
+
+void launch_bc15_encode(int variant, const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                        cudaStream_t s) {
+    if (bw == 0 || bh == 0) return;
+    bool asrc = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
+    size_t bb = (variant == BC_BC1 || variant == BC_BC4) ? 8 : 16;
+    bool adst = ((uintptr_t)dst % bb) == 0;
+    switch (variant) {
+        case BC_BC1: launch_encode<BC_BC1>(src, stride, bw, bh, dst, asrc, adst, s); break;
+        case BC_BC2: launch_encode<BC_BC2>(src, stride, bw, bh, dst, asrc, adst, s); break;
+        case BC_BC3: launch_encode<BC_BC3>(src, stride, bw, bh, dst, asrc, adst, s); break;
+        case BC_BC4: launch_encode<BC_BC4>(src, stride, bw, bh, dst, asrc, adst, s); break;
+        default: launch_encode<BC_BC5>(src, stride, bw, bh, dst, asrc, adst, s); break;
+    }
+}
+
+void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch,
+                        cudaStream_t s) {
+    if (bw == 0 || bh == 0) return;
+    size_t bb = (variant == BC_BC1 || variant == BC_BC4) ? 8 : 16;
+    bool aligned = ((uintptr_t)blocks % bb == 0) && ((uintptr_t)out % 16 == 0) && (pitch % 16 == 0);
+    int g = grid_for(bw * bh, 128);
+    switch (variant) {
+        case BC_BC1: bc15_decode_kernel<BC_BC1><<<g, 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned); break;
+        case BC_BC2: bc15_decode_kernel<BC_BC2><<<g, 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned); break;
+        case BC_BC3: bc15_decode_kernel<BC_BC3><<<g, 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned); break;
+        case BC_BC4: bc15_decode_kernel<BC_BC4><<<g, 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned); break;
+        default: bc15_decode_kernel<BC_BC5><<<g, 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned); break;
+    }
+}
+
+}  // namespace bcn

@@ -1,0 +1,464 @@
+// BC6H and BC7 decode kernels for sm_100a (bit-exact restatement of the
+// reference decoders, src/decode/block.rs:262-1403, and of the image drivers'
+// output layouts, src/decode.rs:151-324).
+//
+// One thread decodes one block; a warp covers 32 neighbouring blocks, so the
+// 16-byte block reads are one contiguous 512-byte span and each output row
+// of the warp is a contiguous span.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "bc_common.cuh"
+#include "bc_kernels.h"
+
+namespace bcn {
+
+// 128-bit little-endian bit reader (block.rs:1341-1403).
+struct Bits128 {
+    uint64_t lo, hi;
+    BCN_DEV uint32_t read(uint32_t n) {
+        uint64_t mask = (1ull << n) - 1;
+        uint32_t b = (uint32_t)(lo & mask);
+        lo = (lo >> n) | ((hi & mask) << (64 - n));
+        hi >>= n;
+        return b;
+    }
+    BCN_DEV int ri(uint32_t n) { return (int)read(n); }
+    BCN_DEV int rev(uint32_t n) {
+        int b = ri(n), r = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            r = (r << 1) | (b & 1);
+            b >>= 1;
+        }
+        return r;
+    }
+};
+
+// Partition-set entry (subset, 0x80 on anchors) derived from the encoder
+// tables; equal to the decoder tables of block.rs:279-312 and :810-947.
+BCN_DEV uint32_t partition_set(uint32_t table_index, uint32_t k) {
+    uint32_t subset = (kPartitionMap[table_index] >> (2 * k)) & 3;
+    uint32_t a = kAnchors[table_index];
+    uint32_t anchor = subset == 0 ? 0 : (subset == 1 ? (a >> 4) : (a & 15));
+    return subset | (k == anchor ? 0x80u : 0u);
+}
+
+BCN_DEV int interp(int a, int b, int w) { return (a * (64 - w) + b * w + 32) >> 6; }
+BCN_DEV int w_of(int bits, int i) {
+    int l1 = (1 << bits) - 1;
+    return (i * 64 + (l1 >> 1)) / l1;
+}
+
+// ---- BC7 (block.rs:801-1252) --------------------------------------------------
+
+BCN_DEV void decode_bc7_block(uint64_t lo, uint64_t hi, uint32_t out[16]) {
+    const uint32_t abits0 = 0x57757564u;  // RGB bits per mode, 4 bits each: 4,6,5,7,5,7,7,5
+    const uint32_t abits1 = 0x57860000u;  // alpha bits per mode: 0,0,0,0,6,8,7,5
+    const uint32_t has_pbits = 0xCB;
+    Bits128 bs{lo, hi};
+    uint32_t mode = 0;
+    while (mode < 8 && bs.read(1) == 0) mode++;
+    if (mode >= 8) {
+        for (int k = 0; k < 16; k++) out[k] = 0;
+        return;
+    }
+    uint32_t cbits = (abits0 >> (4 * mode)) & 15, abits = (abits1 >> (4 * mode)) & 15;
+    uint32_t partition = 0, nparts = 1, rotation = 0, isb = 0;
+    if (mode == 0 || mode == 1 || mode == 2 || mode == 3 || mode == 7) {
+        nparts = (mode == 0 || mode == 2) ? 3 : 2;
+        partition = bs.read(mode == 0 ? 4 : 6);
+    }
+    uint32_t nep = nparts * 2;
+    if (mode == 4 || mode == 5) {
+        rotation = bs.read(2);
+        if (mode == 4) isb = bs.read(1);
+    }
+    int ep[6][4];
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) ep[j][c] = 0;
+    for (int c = 0; c < 3; c++)
+        for (uint32_t j = 0; j < nep; j++) {
+            int v = (int)bs.read(cbits);
+#pragma unroll
+            for (int jj = 0; jj < 6; jj++)
+                if (jj == (int)j) ep[jj][c] = v;
+        }
+    if (abits > 0)
+        for (uint32_t j = 0; j < nep; j++) {
+            int v = (int)bs.read(abits);
+#pragma unroll
+            for (int jj = 0; jj < 6; jj++)
+                if (jj == (int)j) ep[jj][3] = v;
+        }
+    uint32_t pb = (has_pbits >> mode) & 1;
+    if (mode == 0 || mode == 1 || mode == 3 || mode == 6 || mode == 7) {
+#pragma unroll
+        for (int j = 0; j < 6; j++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) ep[j][c] <<= 1;
+        if (mode == 1) {
+            int i0 = (int)bs.read(1), j0 = (int)bs.read(1);
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                ep[0][c] |= i0;
+                ep[1][c] |= i0;
+                ep[2][c] |= j0;
+                ep[3][c] |= j0;
+            }
+        } else if (pb) {
+            for (uint32_t j = 0; j < nep; j++) {
+                int b = (int)bs.read(1);
+#pragma unroll
+                for (int jj = 0; jj < 6; jj++)
+                    if (jj == (int)j)
+#pragma unroll
+                        for (int c = 0; c < 4; c++) ep[jj][c] |= b;
+            }
+        }
+    }
+    {
+        uint32_t jc = cbits + pb, ja = abits + pb;
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                ep[j][c] <<= 8 - jc;
+                ep[j][c] |= ep[j][c] >> jc;
+            }
+            ep[j][3] <<= 8 - ja;
+            ep[j][3] |= ep[j][3] >> ja;
+            if (abits == 0) ep[j][3] = 0xFF;
+        }
+    }
+    uint32_t ib = (mode == 0 || mode == 1) ? 3 : (mode == 6 ? 4 : 2);
+    uint32_t ib2 = mode == 4 ? 3 : (mode == 5 ? 2 : 0);
+    uint32_t table = nparts == 3 ? 64 + partition : partition;
+    uint32_t idx[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        uint32_t ps = nparts == 1 ? (k == 0 ? 0x80u : 0u) : partition_set(table, k);
+        idx[k] = bs.read((ps & 0x80) ? ib - 1 : ib);
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        uint32_t s = nparts == 1 ? 0u : (partition_set(table, k) & 3);
+        const int* e0 = s == 0 ? ep[0] : (s == 1 ? ep[2] : ep[4]);
+        const int* e1 = s == 0 ? ep[1] : (s == 1 ? ep[3] : ep[5]);
+        int r, g, b, a;
+        int w = w_of((int)ib, (int)idx[k]);
+        if (ib2 == 0) {
+            r = interp(e0[0], e1[0], w);
+            g = interp(e0[1], e1[1], w);
+            b = interp(e0[2], e1[2], w);
+            a = interp(e0[3], e1[3], w);
+        } else {
+            int i2 = (int)bs.read(k == 0 ? ib2 - 1 : ib2);
+            int w2 = w_of((int)ib2, i2);
+            if (isb == 0) {
+                r = interp(e0[0], e1[0], w);
+                g = interp(e0[1], e1[1], w);
+                b = interp(e0[2], e1[2], w);
+                a = interp(e0[3], e1[3], w2);
+            } else {
+                r = interp(e0[0], e1[0], w2);
+                g = interp(e0[1], e1[1], w2);
+                b = interp(e0[2], e1[2], w2);
+                a = interp(e0[3], e1[3], w);
+            }
+        }
+        int t;
+        if (rotation == 1) {
+            t = a;
+            a = r;
+            r = t;
+        } else if (rotation == 2) {
+            t = a;
+            a = g;
+            g = t;
+        } else if (rotation == 3) {
+            t = a;
+            a = b;
+            b = t;
+        }
+        out[k] = (uint32_t)(r & 0xFF) | ((uint32_t)(g & 0xFF) << 8) | ((uint32_t)(b & 0xFF) << 16) |
+                 ((uint32_t)(a & 0xFF) << 24);
+    }
+}
+
+__global__ void __launch_bounds__(128) bc7_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
+                                                         uint8_t* __restrict__ out, size_t pitch, bool aligned) {
+    uint32_t n = bw * bh;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t by = i / bw, bx = i - by * bw;
+        uint64_t lo = 0, hi = 0;
+        const uint8_t* b = blocks + (size_t)i * 16;
+        if (aligned) {
+            uint4 v = __ldg(reinterpret_cast<const uint4*>(b));
+            lo = (uint64_t)v.x | ((uint64_t)v.y << 32);
+            hi = (uint64_t)v.z | ((uint64_t)v.w << 32);
+        } else {
+            for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+            for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        }
+        uint32_t px[16];
+        decode_bc7_block(lo, hi, px);
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            uint8_t* row = out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
+            if (aligned) {
+                *reinterpret_cast<uint4*>(row) = make_uint4(px[y * 4], px[y * 4 + 1], px[y * 4 + 2], px[y * 4 + 3]);
+            } else {
+                for (int x = 0; x < 4; x++)
+                    for (int c = 0; c < 4; c++) row[4 * x + c] = (uint8_t)(px[y * 4 + x] >> (8 * c));
+            }
+        }
+    }
+}
+
+// ---- BC6H (block.rs:262-796) -----------------------------------------------------
+
+BCN_DEV int extend_sign(int v, int bits) { return (int)((uint32_t)v << (32 - bits)) >> (32 - bits); }
+
+BCN_DEV int unquantize_u(int v, int bits) {
+    if (bits >= 15) return v;
+    if (v == 0) return 0;
+    if (v == (1 << bits) - 1) return 0xFFFF;
+    return ((v << 16) + 0x8000) >> bits;
+}
+
+// Unsigned BC6H (the only form the image drivers use): 16 pixels of RGB
+// f16 bit patterns.
+BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
+    Bits128 bs{lo, hi};
+    int r[4] = {0, 0, 0, 0}, g[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
+    uint32_t mode = bs.read(2);
+    if (mode > 1) mode |= bs.read(3) << 2;
+    int part = 0;
+    switch (mode) {
+        case 0x00:
+            g[2] |= bs.ri(1) << 4; b[2] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 4;
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
+            g[1] |= bs.ri(5); b[3] |= bs.ri(1); g[3] |= bs.ri(4);
+            b[1] |= bs.ri(5); b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4);
+            r[2] |= bs.ri(5); b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 0;
+            break;
+        case 0x01:
+            g[2] |= bs.ri(1) << 5; g[3] |= bs.ri(1) << 4; g[3] |= bs.ri(1) << 5;
+            r[0] |= bs.ri(7); b[3] |= bs.ri(1); b[3] |= bs.ri(1) << 1;
+            b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(7); b[2] |= bs.ri(1) << 5;
+            b[3] |= bs.ri(1) << 2; g[2] |= bs.ri(1) << 4; b[0] |= bs.ri(7);
+            b[3] |= bs.ri(1) << 3; b[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(6); g[2] |= bs.ri(4); g[1] |= bs.ri(6);
+            g[3] |= bs.ri(4); b[1] |= bs.ri(6); b[2] |= bs.ri(4);
+            r[2] |= bs.ri(6); r[3] |= bs.ri(6); part = bs.ri(5); mode = 1;
+            break;
+        case 0x02:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(5); r[0] |= bs.ri(1) << 10; g[2] |= bs.ri(4);
+            g[1] |= bs.ri(4); g[0] |= bs.ri(1) << 10; b[3] |= bs.ri(1);
+            g[3] |= bs.ri(4); b[1] |= bs.ri(4); b[0] |= bs.ri(1) << 10;
+            b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4); r[2] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(5); b[3] |= bs.ri(1) << 3;
+            part = bs.ri(5); mode = 2;
+            break;
+        case 0x06:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(4); r[0] |= bs.ri(1) << 10; g[3] |= bs.ri(1) << 4;
+            g[2] |= bs.ri(4); g[1] |= bs.ri(5); g[0] |= bs.ri(1) << 10;
+            g[3] |= bs.ri(4); b[1] |= bs.ri(4); b[0] |= bs.ri(1) << 10;
+            b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4); r[2] |= bs.ri(4);
+            b[3] |= bs.ri(1); b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(4);
+            g[2] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 3;
+            break;
+        case 0x0A:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(4); r[0] |= bs.ri(1) << 10; b[2] |= bs.ri(1) << 4;
+            g[2] |= bs.ri(4); g[1] |= bs.ri(4); g[0] |= bs.ri(1) << 10;
+            b[3] |= bs.ri(1); g[3] |= bs.ri(4); b[1] |= bs.ri(5);
+            b[0] |= bs.ri(1) << 10; b[2] |= bs.ri(4); r[2] |= bs.ri(4);
+            b[3] |= bs.ri(1) << 1; b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(4);
+            b[3] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 4;
+            break;
+        case 0x0E:
+            r[0] |= bs.ri(9); b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(9);
+            g[2] |= bs.ri(1) << 4; b[0] |= bs.ri(9); b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
+            g[1] |= bs.ri(5); b[3] |= bs.ri(1); g[3] |= bs.ri(4);
+            b[1] |= bs.ri(5); b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4);
+            r[2] |= bs.ri(5); b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 5;
+            break;
+        case 0x12:
+            r[0] |= bs.ri(8); g[3] |= bs.ri(1) << 4; b[2] |= bs.ri(1) << 4;
+            g[0] |= bs.ri(8); b[3] |= bs.ri(1) << 2; g[2] |= bs.ri(1) << 4;
+            b[0] |= bs.ri(8); b[3] |= bs.ri(1) << 3; b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(6); g[2] |= bs.ri(4); g[1] |= bs.ri(5);
+            b[3] |= bs.ri(1); g[3] |= bs.ri(4); b[1] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4); r[2] |= bs.ri(6);
+            r[3] |= bs.ri(6); part = bs.ri(5); mode = 6;
+            break;
+        case 0x16:
+            r[0] |= bs.ri(8); b[3] |= bs.ri(1); b[2] |= bs.ri(1) << 4;
+            g[0] |= bs.ri(8); g[2] |= bs.ri(1) << 5; g[2] |= bs.ri(1) << 4;
+            b[0] |= bs.ri(8); g[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
+            g[1] |= bs.ri(6); g[3] |= bs.ri(4); b[1] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(4); r[2] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(5); b[3] |= bs.ri(1) << 3;
+            part = bs.ri(5); mode = 7;
+            break;
+        case 0x1A:
+            r[0] |= bs.ri(8); b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(1) << 4;
+            g[0] |= bs.ri(8); b[2] |= bs.ri(1) << 5; g[2] |= bs.ri(1) << 4;
+            b[0] |= bs.ri(8); b[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
+            g[1] |= bs.ri(5); b[3] |= bs.ri(1); g[3] |= bs.ri(4);
+            b[1] |= bs.ri(6); b[2] |= bs.ri(4); r[2] |= bs.ri(5);
+            b[3] |= bs.ri(1) << 2; r[3] |= bs.ri(5); b[3] |= bs.ri(1) << 3;
+            part = bs.ri(5); mode = 8;
+            break;
+        case 0x1E:
+            r[0] |= bs.ri(6); g[3] |= bs.ri(1) << 4; b[3] |= bs.ri(1);
+            b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(6);
+            g[2] |= bs.ri(1) << 5; b[2] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 2;
+            g[2] |= bs.ri(1) << 4; b[0] |= bs.ri(6); g[3] |= bs.ri(1) << 5;
+            b[3] |= bs.ri(1) << 3; b[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
+            r[1] |= bs.ri(6); g[2] |= bs.ri(4); g[1] |= bs.ri(6);
+            g[3] |= bs.ri(4); b[1] |= bs.ri(6); b[2] |= bs.ri(4);
+            r[2] |= bs.ri(6); r[3] |= bs.ri(6); part = bs.ri(5); mode = 9;
+            break;
+        case 0x03:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(10); g[1] |= bs.ri(10); b[1] |= bs.ri(10);
+            mode = 10;
+            break;
+        case 0x07:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(9); r[0] |= bs.ri(1) << 10; g[1] |= bs.ri(9);
+            g[0] |= bs.ri(1) << 10; b[1] |= bs.ri(9); b[0] |= bs.ri(1) << 10;
+            mode = 11;
+            break;
+        case 0x0B:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(8); r[0] |= bs.rev(2) << 10; g[1] |= bs.ri(8);
+            g[0] |= bs.rev(2) << 10; b[1] |= bs.ri(8); b[0] |= bs.rev(2) << 10;
+            mode = 12;
+            break;
+        case 0x0F:
+            r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
+            r[1] |= bs.ri(4); r[0] |= bs.rev(6) << 10; g[1] |= bs.ri(4);
+            g[0] |= bs.rev(6) << 10; b[1] |= bs.ri(4); b[0] |= bs.rev(6) << 10;
+            mode = 13;
+            break;
+        default:
+            for (int i = 0; i < 48; i++) out[i] = 0;
+            return;
+    }
+    // ACTUAL_BITS_COUNT (block.rs:269-274)
+    const uint8_t kB0[14] = {10, 7, 11, 11, 11, 9, 8, 8, 8, 6, 10, 11, 12, 16};
+    const uint8_t kBR[14] = {5, 6, 5, 4, 4, 5, 6, 5, 5, 6, 10, 9, 8, 4};
+    const uint8_t kBG[14] = {5, 6, 4, 5, 4, 5, 5, 6, 5, 6, 10, 9, 8, 4};
+    const uint8_t kBB[14] = {5, 6, 4, 4, 5, 5, 5, 5, 6, 6, 10, 9, 8, 4};
+    int np = mode >= 10 ? 0 : 1;
+    int bits0 = kB0[mode];
+    if (mode != 9 && mode != 10) {
+        for (int i = 1; i < (np + 1) * 2; i++) {
+            int rr = extend_sign(i == 1 ? r[1] : (i == 2 ? r[2] : r[3]), kBR[mode]);
+            int gg = extend_sign(i == 1 ? g[1] : (i == 2 ? g[2] : g[3]), kBG[mode]);
+            int bb = extend_sign(i == 1 ? b[1] : (i == 2 ? b[2] : b[3]), kBB[mode]);
+            int m = (1 << bits0) - 1;
+            rr = (rr + r[0]) & m;
+            gg = (gg + g[0]) & m;
+            bb = (bb + b[0]) & m;
+            if (i == 1) { r[1] = rr; g[1] = gg; b[1] = bb; }
+            else if (i == 2) { r[2] = rr; g[2] = gg; b[2] = bb; }
+            else { r[3] = rr; g[3] = gg; b[3] = bb; }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (i >= (np + 1) * 2) break;
+        r[i] = unquantize_u(r[i], bits0);
+        g[i] = unquantize_u(g[i], bits0);
+        b[i] = unquantize_u(b[i], bits0);
+    }
+    int ib = mode >= 10 ? 4 : 3;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        uint32_t ps = mode >= 10 ? (k == 0 ? 0x80u : 0u) : partition_set((uint32_t)part, k);
+        int nb = (ps & 0x80) ? ib - 1 : ib;
+        int idx = bs.ri(nb);
+        int e = (ps & 1) ? 2 : 0;
+        int w = w_of(ib, idx);
+        int r0 = e ? r[2] : r[0], r1 = e ? r[3] : r[1];
+        int g0 = e ? g[2] : g[0], g1 = e ? g[3] : g[1];
+        int b0 = e ? b[2] : b[0], b1 = e ? b[3] : b[1];
+        out[k * 3 + 0] = (uint16_t)((interp(r0, r1, w) * 31) >> 6);
+        out[k * 3 + 1] = (uint16_t)((interp(g0, g1, w) * 31) >> 6);
+        out[k * 3 + 2] = (uint16_t)((interp(b0, b1, w) * 31) >> 6);
+    }
+}
+
+// f16 (non-negative, finite: the unsigned decoder never produces more than
+// 0x7BFF) -> sRGB u8, the reference's linear_to_srgb (decode.rs:151-159)
+// evaluated on the host for every such bit pattern.
+__device__ uint8_t g_half_to_srgb[0x7C00];
+
+__global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
+                                                          void* __restrict__ out, size_t pitch, int fmt) {
+    uint32_t n = bw * bh;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t by = i / bw, bx = i - by * bw;
+        const uint8_t* b = blocks + (size_t)i * 16;
+        uint64_t lo = 0, hi = 0;
+        for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+        for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        uint16_t h[48];
+        decode_bc6h_block_u(lo, hi, h);
+        for (int y = 0; y < 4; y++) {
+            size_t row = (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
+            if (fmt == 0) {
+                uint8_t* o = reinterpret_cast<uint8_t*>(out) + row;
+                for (int x = 0; x < 4; x++) {
+                    for (int c = 0; c < 3; c++) o[4 * x + c] = g_half_to_srgb[min((int)h[(y * 4 + x) * 3 + c], 0x7BFF)];
+                    o[4 * x + 3] = 0;
+                }
+            } else if (fmt == 1) {
+                uint16_t* o = reinterpret_cast<uint16_t*>(out) + row;
+                for (int j = 0; j < 12; j++) o[j] = h[y * 12 + j];
+            } else {
+                float* o = reinterpret_cast<float*>(out) + row;
+                for (int j = 0; j < 12; j++) o[j] = __half2float(__ushort_as_half(h[y * 12 + j]));
+            }
+        }
+    }
+}
+
+static int grid_for(uint32_t n) {
+    uint32_t g = (n + 127) / 128;
+    return (int)(g > 148u * 64u ? 148u * 64u : (g == 0 ? 1 : g));
+}
+
+void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s) {
+    if (bw == 0 || bh == 0) return;
+    bool aligned = ((uintptr_t)blocks % 16 == 0) && ((uintptr_t)out % 16 == 0) && (pitch % 16 == 0);
+    bc7_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned);
+}
+
+void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
+                        cudaStream_t s) {
+    if (bw == 0 || bh == 0) return;
+    bc6h_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, out_format);
+}
+
+}  // namespace bcn
+
+namespace bcn {
+cudaError_t set_half_to_srgb_table(const uint8_t* host) {
+    return cudaMemcpyToSymbol(g_half_to_srgb, host, sizeof(g_half_to_srgb));
+}
+}  // namespace bcn

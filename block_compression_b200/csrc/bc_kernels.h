@@ -1,0 +1,51 @@
+// Internal launcher declarations shared by the kernel translation units and
+// the C-ABI layer (capi.cu). Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace bcn {
+
+// Variant ids: order of the reference enum CompressionVariant (src/lib.rs:74-103).
+enum Variant { BC_BC1 = 0, BC_BC2 = 1, BC_BC3 = 2, BC_BC4 = 3, BC_BC5 = 4, BC_BC6H = 5, BC_BC7 = 6 };
+
+// Settings with the byte layout of the reference's #[repr(C)] structs
+// (src/settings.rs:207-213, :278-288).
+struct BC6HSettingsDev {
+    uint32_t slow_mode, fast_mode, refine_iterations_1p, refine_iterations_2p, fast_skip_threshold;
+};
+struct BC7SettingsDev {
+    uint32_t refine_iterations[8];
+    uint32_t mode_selection[4];
+    uint32_t skip_mode2, fast_skip_threshold_mode1, fast_skip_threshold_mode3, fast_skip_threshold_mode7;
+    uint32_t mode45_channel0, refine_iterations_channel, channels;
+};
+
+// Source pixel formats a BC6H launch can read.
+enum Bc6hSource { BC6H_SRC_RGBA16F = 0, BC6H_SRC_RGBA8_SRGB = 1 };
+
+void launch_bc15_encode(int variant, const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                        cudaStream_t s);
+void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch,
+                        cudaStream_t s);
+void launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                       const BC7SettingsDev& settings, cudaStream_t s);
+void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s);
+// stride in bytes of the source rows (RGBA16F: 8 bytes per pixel; RGBA8: 4).
+void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,
+                        uint8_t* dst, const BC6HSettingsDev& settings, cudaStream_t s);
+// out_format: 0 RGBA8 (sRGB-encoded), 1 RGBA16F (RGB triplets in RGBA rows),
+// 2 RGBA32F (same layout); pitch in output elements.
+void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
+                        cudaStream_t s);
+
+// One-time per-device table upload (sRGB conversion LUTs computed on the host).
+int upload_bc6h_tables();
+// Copies a host table into the device symbol of the translation unit that
+// owns it (0x7C00 entries: f16 bits -> sRGB u8; 256 entries: u8 -> f16 bits).
+cudaError_t set_half_to_srgb_table(const uint8_t* host);
+cudaError_t set_srgb_to_half_table(const uint16_t* host);
+
+}  // namespace bcn

@@ -1,0 +1,298 @@
+// Shared float math of the BC6H and BC7 encoders (the reference's
+// src/encode/common.rs), written for the tiled kernels: a block is read
+// through a view object (planar, lane-strided shared memory), and every sum
+// keeps the reference's operation order so results are bit-identical.
+#pragma once
+#include "bc_common.cuh"
+
+namespace bcn {
+namespace bptc {
+
+constexpr int NB = 32;  // blocks per tile; lane l of each warp owns block l
+
+// Planar view of one block in shared memory: channel c, pixel k.
+struct Blk {
+    const float* p;
+    BCN_DEV float operator()(int c, int k) const { return p[(c * 16 + k) * NB]; }
+};
+
+// ---- shared math (src/encode/common.rs) -------------------------------------
+
+BCN_DEV int unquant_w(int bits, int i) {
+    // (i*64 + (L-1)/2) / (L-1), L = 2^bits: equals the reference table
+    // get_unquant_value (common.rs:6-21) for every index.
+    int l1 = (1 << bits) - 1;
+    return (i * 64 + (l1 >> 1)) / l1;
+}
+
+BCN_DEV float sel3(int j, float a, float b, float c) { return j == 0 ? a : (j == 1 ? b : c); }
+
+// common.rs:294-332 over the set pixels only (adding the reference's +0.0
+// terms of unset pixels changes none of the non-negative sums).
+template <int CH, class B>
+BCN_DEV void stats_masked(const B& blk, uint32_t mask, float st[15]) {
+#pragma unroll
+    for (int i = 0; i < 15; i++) st[i] = 0.0f;
+    for (uint32_t m = mask & 0xFFFFu; m; m &= m - 1) {
+        int k = __ffs(m) - 1;
+        float r = blk(0, k), g = blk(1, k), b = blk(2, k);
+        st[14] += 1.0f;
+        st[10] += r;
+        st[11] += g;
+        st[12] += b;
+        st[0] += r * r;
+        st[1] += r * g;
+        st[2] += r * b;
+        st[4] += g * g;
+        st[5] += g * b;
+        st[7] += b * b;
+        if (CH == 4) {
+            float a = blk(3, k);
+            st[13] += a;
+            st[3] += r * a;
+            st[6] += g * a;
+            st[8] += b * a;
+            st[9] += a * a;
+        }
+    }
+}
+
+// common.rs:334-350 (entries of a 3-channel call outside its 6 stay 0)
+template <int CH>
+BCN_DEV void covar_from_stats(float cv[10], const float st[15]) {
+    cv[0] = st[0] - st[10] * st[10] / st[14];
+    cv[1] = st[1] - st[10] * st[11] / st[14];
+    cv[2] = st[2] - st[10] * st[12] / st[14];
+    cv[4] = st[4] - st[11] * st[11] / st[14];
+    cv[5] = st[5] - st[11] * st[12] / st[14];
+    cv[7] = st[7] - st[12] * st[12] / st[14];
+    if (CH == 4) {
+        cv[3] = st[3] - st[10] * st[13] / st[14];
+        cv[6] = st[6] - st[11] * st[13] / st[14];
+        cv[8] = st[8] - st[12] * st[13] / st[14];
+        cv[9] = st[9] - st[13] * st[13] / st[14];
+    } else {
+        cv[3] = cv[6] = cv[8] = cv[9] = 0.0f;
+    }
+}
+
+template <int CH>
+BCN_DEV void ssymv(float a[4], const float c[10], const float b[4]) {
+    if (CH == 3) {
+        a[0] = c[0] * b[0] + c[1] * b[1] + c[2] * b[2];
+        a[1] = c[1] * b[0] + c[4] * b[1] + c[5] * b[2];
+        a[2] = c[2] * b[0] + c[5] * b[1] + c[7] * b[2];
+    } else {
+        a[0] = c[0] * b[0] + c[1] * b[1] + c[2] * b[2] + c[3] * b[3];
+        a[1] = c[1] * b[0] + c[4] * b[1] + c[5] * b[2] + c[6] * b[3];
+        a[2] = c[2] * b[0] + c[5] * b[1] + c[7] * b[2] + c[8] * b[3];
+        a[3] = c[3] * b[0] + c[6] * b[1] + c[8] * b[2] + c[9] * b[3];
+    }
+}
+
+// common.rs:260-292
+template <int CH, int ITERS>
+BCN_DEV void compute_axis(float axis[4], const float cv[10]) {
+    float a[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+#pragma unroll
+    for (int i = 0; i < ITERS; i++) {
+        ssymv<CH>(axis, cv, a);
+#pragma unroll
+        for (int p = 0; p < CH; p++) a[p] = axis[p];
+        if (i % 2 == 1) {
+            float n = 0.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) n += sqf(axis[p]);
+            float rn = 1.0f / sqrtf(n);
+#pragma unroll
+            for (int p = 0; p < CH; p++) a[p] *= rn;
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < CH; p++) axis[p] = a[p];
+}
+
+// common.rs:208-245
+template <int CH>
+BCN_DEV float pca_bound(const float cv[10]) {
+    float cs[10];
+    const float inv_var = 1.0f / 65536.0f;
+#pragma unroll
+    for (int i = 0; i < 10; i++) cs[i] = cv[i] * inv_var;
+    const float eps = 0.001f * 0.001f;
+    cs[0] += eps;
+    cs[4] += eps;
+    cs[7] += eps;
+    float axis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    compute_axis<CH, 4>(axis, cs);
+    float av[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    ssymv<CH>(av, cs, axis);
+    float s = 0.0f;
+#pragma unroll
+    for (int p = 0; p < CH; p++) s += sqf(av[p]);
+    float lambda = sqrtf(s);
+    float bound = cs[0] + cs[4] + cs[7];
+    if (CH == 4) bound += cs[9];
+    bound -= lambda;
+    return fmaxf(bound, 0.0f);
+}
+
+// common.rs:396-420
+template <int CH>
+BCN_DEV float pca_bound_split(const Blk& blk, uint32_t mask, const float full[15]) {
+    float st[15], cv[10];
+    stats_masked<CH>(blk, mask, st);
+    covar_from_stats<CH>(cv, st);
+    float b = 0.0f;
+    b += pca_bound<CH>(cv);
+#pragma unroll
+    for (int i = 0; i < 15; i++) st[i] = full[i] - st[i];
+    covar_from_stats<CH>(cv, st);
+    b += pca_bound<CH>(cv);
+    return sqrtf(b) * 256.0f;
+}
+
+// common.rs:483-518 (+ bc7.rs:371-379 clamp when CLAMP)
+template <int CH, bool CLAMP, class B>
+BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
+    float st[15], cv[10], dc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, axis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    stats_masked<CH>(blk, mask, st);
+#pragma unroll
+    for (int p = 0; p < CH; p++) dc[p] = st[10 + p] / st[14];
+    covar_from_stats<CH>(cv, st);
+    const float inv_var = 1.0f / 65536.0f;
+#pragma unroll
+    for (int i = 0; i < 10; i++) cv[i] *= inv_var;
+    const float eps = 0.001f * 0.001f;
+    cv[0] += eps;
+    cv[4] += eps;
+    cv[7] += eps;
+    cv[9] += eps;
+    compute_axis<CH, 8>(axis, cv);
+    float e0 = __int_as_float(0x7f800000), e1 = __int_as_float(0xff800000);
+    for (uint32_t m = mask & 0xFFFFu; m; m &= m - 1) {
+        int k = __ffs(m) - 1;
+        float dot = 0.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) dot += axis[p] * (blk(p, k) - dc[p]);
+        e0 = fminf(e0, dot);
+        e1 = fmaxf(e1, dot);
+    }
+    if (e1 - e0 < 1.0f) {
+        e0 -= 0.5f;
+        e1 += 0.5f;
+    }
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        float a = e0 * axis[p] + dc[p];
+        float b = e1 * axis[p] + dc[p];
+        if (CLAMP) {
+            a = clampf_r(a, 0.0f, 255.0f);
+            b = clampf_r(b, 0.0f, 255.0f);
+        }
+        ep[p] = a;
+        ep[4 + p] = b;
+    }
+}
+
+// common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8.
+template <int CH, int BITS, int PAIRS, class B>
+BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
+    constexpr int levels = 1 << BITS;
+    float total = 0.0f;
+    q0 = 0;
+    q1 = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        int j = PAIRS == 1 ? 0 : (int)((pattern >> (2 * k)) & 3);
+        float ea[CH], eb[CH];
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            ea[p] = PAIRS == 1 ? ep[p] : (PAIRS == 2 ? (j == 0 ? ep[p] : ep[8 + p]) : sel3(j, ep[p], ep[8 + p], ep[16 + p]));
+            eb[p] = PAIRS == 1 ? ep[4 + p]
+                               : (PAIRS == 2 ? (j == 0 ? ep[4 + p] : ep[12 + p]) : sel3(j, ep[4 + p], ep[12 + p], ep[20 + p]));
+        }
+        float proj = 0.0f, div = 0.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            float v = blk(p, k);
+            proj += (v - ea[p]) * (eb[p] - ea[p]);
+            div += sqf(eb[p] - ea[p]);
+        }
+        proj /= div;
+        int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
+        int w0 = unquant_w(BITS, q1i - 1), w1 = unquant_w(BITS, q1i);
+        float err0 = 0.0f, err1 = 0.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            int ia = (int)ea[p], ib = (int)eb[p];
+            float v = blk(p, k);
+            float d0 = (float)(((64 - w0) * ia + w0 * ib + 32) / 64);
+            float d1 = (float)(((64 - w1) * ia + w1 * ib + 32) / 64);
+            err0 += sqf(d0 - v);
+            err1 += sqf(d1 - v);
+        }
+        float be = err1;
+        int bq = q1i;
+        if (err0 < err1) {
+            be = err0;
+            bq = q1i - 1;
+        }
+        if (k < 8) q0 |= (uint32_t)bq << (4 * k);
+        else q1 |= (uint32_t)bq << (4 * (k - 8));
+        total += be;
+    }
+    return total;
+}
+
+// common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH).
+template <int CH, int BITS, class B>
+BCN_DEV void opt_endpoints(float* ep, const B& blk, uint32_t q0, uint32_t q1, uint32_t mask) {
+    constexpr int levels = 1 << BITS;
+    const float lm1 = (float)(levels - 1);
+    float atb1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sum[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float sum_q = 0.0f, sum_qq = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        float q = (float)(((k < 8 ? q0 : q1) >> (4 * (k & 7))) & 15);
+        if (((mask >> k) & 1) == 0) continue;
+        float x = lm1 - q;
+        sum_q += q;
+        sum_qq += q * q;
+        sum[4] += 1.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            float v = blk(p, k);
+            sum[p] += v;
+            atb1[p] += x * v;
+        }
+    }
+    float atb2[4];
+#pragma unroll
+    for (int p = 0; p < CH; p++) atb2[p] = lm1 * sum[p] - atb1[p];
+    float cxx = sum[4] * sqf(lm1) - 2.0f * lm1 * sum_q + sum_qq;
+    float cyy = sum_qq;
+    float cxy = lm1 * sum_q - sum_qq;
+    float det = cxx * cyy - cxy * cxy;
+    float scale = lm1 / det;
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        ep[p] = (atb1[p] * cyy - atb2[p] * cxy) * scale;
+        ep[4 + p] = (atb2[p] * cxx - atb1[p] * cxy) * scale;
+    }
+    if (fabsf(det) < 0.001f) {
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            ep[p] = sum[p] / sum[4];
+            ep[4 + p] = ep[p];
+        }
+    }
+}
+
+BCN_DEV int unpack_to_byte(int v, int bits) {
+    int vv = v << (8 - bits);
+    return vv + (vv >> bits);
+}
+
+}  // namespace bptc
+}  // namespace bcn

@@ -1,0 +1,175 @@
+/* bc_capi.h — C ABI of the B200 (sm_100a) BCn block-compression library.
+ *
+ * Drop-in boundary for the per-4x4-block BCn codec of the Rust crate
+ * block_compression v0.3.0 (novacrazy/block_compression). Every entry point
+ * below names the reference interface it replaces. A Rust shim binds these
+ * symbols with `extern "C"` and turns a negative status into the same panic
+ * the reference raises (INTEGRATION.md shows the binding).
+ *
+ * Conventions
+ *   - Every function returns an int status: BC_OK (0) or a negative BC_ERR_*.
+ *     Nothing aborts the process.
+ *   - `stream` arguments are cudaStream_t values passed as void* (NULL = the
+ *     legacy default stream). *_device entry points are stream-ordered and
+ *     asynchronous: they validate arguments, enqueue kernels and return.
+ *   - Host-pointer entry points (bc_compress_rgba8, ...) are synchronous and
+ *     mirror the reference's CPU functions byte for byte.
+ *   - Output blocks are little-endian, in row-major block order, exactly as
+ *     the reference writes them (src/encode.rs store_data).
+ *   - All work runs on the CUDA device current on the calling thread.
+ */
+#ifndef BC_CAPI_H
+#define BC_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define BC_OK 0
+#define BC_ERR_DIMS -1          /* width/height/y-offset not a multiple of 4 (src/encode.rs:91-92) */
+#define BC_ERR_DST_SIZE -2      /* destination too small / not the expected size (src/encode.rs:96-101) */
+#define BC_ERR_SRC_SIZE -3      /* source buffer shorter than the rows it must cover */
+#define BC_ERR_VARIANT -4       /* variant not valid for this entry point (src/encode.rs:247-249) */
+#define BC_ERR_SETTINGS -5      /* settings outside the range the reference can run */
+#define BC_ERR_NULL -6          /* required pointer is NULL */
+#define BC_ERR_CUDA -7          /* a CUDA runtime call failed (bc_last_cuda_error() has the code) */
+#define BC_ERR_TASKS -8         /* task queue full / empty handle */
+#define BC_ERR_NO_DEVICE -9     /* no usable sm_100 device */
+
+/* ---- variants: order of CompressionVariant (src/lib.rs:74-103) ------------ */
+typedef enum bc_variant {
+    BC_VARIANT_BC1 = 0,
+    BC_VARIANT_BC2 = 1,
+    BC_VARIANT_BC3 = 2,
+    BC_VARIANT_BC4 = 3,
+    BC_VARIANT_BC5 = 4,
+    BC_VARIANT_BC6H = 5,
+    BC_VARIANT_BC7 = 6
+} bc_variant;
+
+/* BC6HSettings, byte layout of the #[repr(C)] struct (src/settings.rs:207-213). */
+typedef struct bc_bc6h_settings {
+    uint32_t slow_mode;
+    uint32_t fast_mode;
+    uint32_t refine_iterations_1p;
+    uint32_t refine_iterations_2p;
+    uint32_t fast_skip_threshold;
+} bc_bc6h_settings;
+
+/* BC7Settings, byte layout of the #[repr(C)] struct (src/settings.rs:278-288). */
+typedef struct bc_bc7_settings {
+    uint32_t refine_iterations[8];
+    uint32_t mode_selection[4];
+    uint32_t skip_mode2;
+    uint32_t fast_skip_threshold_mode1;
+    uint32_t fast_skip_threshold_mode3;
+    uint32_t fast_skip_threshold_mode7;
+    uint32_t mode45_channel0;
+    uint32_t refine_iterations_channel;
+    uint32_t channels;
+} bc_bc7_settings;
+
+/* Quality presets (src/settings.rs:217-441). `name` is the reference
+ * constructor name, e.g. "basic", "alpha_basic", "opaque_ultra_fast".
+ * Returns BC_ERR_SETTINGS for an unknown name. */
+int bc_bc6h_settings_preset(const char* name, bc_bc6h_settings* out);
+int bc_bc7_settings_preset(const char* name, bc_bc7_settings* out);
+
+/* ---- sizes (CompressionVariant::bytes_per_row / blocks_byte_size, src/lib.rs:129-157) */
+uint32_t bc_bytes_per_row(int variant, uint32_t width);
+size_t bc_blocks_byte_size(int variant, uint32_t width, uint32_t height);
+
+/* ---- encode, host buffers (synchronous) ---------------------------------
+ * encode::compress_rgba8 (src/encode.rs:83-151). `settings` points to a
+ * bc_bc6h_settings for BC6H, a bc_bc7_settings for BC7, and is ignored (may be
+ * NULL) for BC1-BC5. stride is in bytes. rgba_len is the length of the
+ * source slice, blocks_len of the destination slice. */
+int bc_compress_rgba8(int variant, const void* settings, const uint8_t* rgba, size_t rgba_len,
+                      uint8_t* blocks, size_t blocks_len, uint32_t width, uint32_t height,
+                      uint32_t stride);
+
+/* encode::compress_rgba16 (src/encode.rs:211-251). `rgba` holds IEEE binary16
+ * values; stride and rgba_len are in f16 elements. variant must be BC6H. */
+int bc_compress_rgba16(int variant, const bc_bc6h_settings* settings, const uint16_t* rgba,
+                       size_t rgba_len, uint8_t* blocks, size_t blocks_len, uint32_t width,
+                       uint32_t height, uint32_t stride);
+
+/* ---- encode, device buffers (stream-ordered) -------------------------------
+ * Same computation on device-resident buffers. Byte strides. */
+int bc_compress_rgba8_device(int variant, const void* settings, const uint8_t* rgba_dev,
+                             size_t rgba_len, uint8_t* blocks_dev, size_t blocks_len,
+                             uint32_t width, uint32_t height, size_t stride_bytes, void* stream);
+int bc_compress_rgba16_device(const bc_bc6h_settings* settings, const uint16_t* rgba_dev,
+                              size_t rgba_len, uint8_t* blocks_dev, size_t blocks_len,
+                              uint32_t width, uint32_t height, size_t stride_elems, void* stream);
+
+/* ---- decode --------------------------------------------------------------
+ * decode::decompress_blocks_as_rgba8 (src/decode.rs:336-387): blocks_len must
+ * equal bc_blocks_byte_size(variant, w, h) and rgba_len must equal w*h*4.
+ * BC4 decodes to (R,0,0,0), BC5 to (R,G,0,0), BC6H to sRGB-encoded RGB with
+ * A=0, as the reference does (src/decode.rs:97-181). */
+int bc_decompress_blocks_as_rgba8(int variant, uint32_t width, uint32_t height,
+                                  const uint8_t* blocks, size_t blocks_len, uint8_t* rgba,
+                                  size_t rgba_len);
+/* decode::decompress_blocks_as_rgba16f / rgba32f (src/decode.rs:397-468), BC6H
+ * only. Like the reference, each pixel's RGB triplet is written at element
+ * (y*width*4 + bx*16 + x*3) of its row, leaving the last 4 elements of every
+ * 16-element block row untouched. out_len is in elements (w*h*4). */
+int bc_decompress_blocks_as_rgba16f(int variant, uint32_t width, uint32_t height,
+                                    const uint8_t* blocks, size_t blocks_len, uint16_t* rgba,
+                                    size_t rgba_len);
+int bc_decompress_blocks_as_rgba32f(int variant, uint32_t width, uint32_t height,
+                                    const uint8_t* blocks, size_t blocks_len, float* rgba,
+                                    size_t rgba_len);
+/* Device-buffer decode, stream-ordered. out_format: 0 RGBA8, 1 RGBA16F, 2 RGBA32F. */
+int bc_decompress_device(int variant, uint32_t width, uint32_t height, const uint8_t* blocks_dev,
+                         size_t blocks_len, void* out_dev, size_t out_len, int out_format,
+                         void* stream);
+
+/* ---- GpuBlockCompressor task interface (src/block_compressor.rs:44-590) ---- */
+typedef struct bc_compressor bc_compressor;
+
+/* GpuBlockCompressor::new (src/block_compressor.rs:66). `device` is a CUDA
+ * device ordinal; -1 uses the current device. */
+int bc_compressor_create(int device, bc_compressor** out);
+int bc_compressor_destroy(bc_compressor* c);
+
+/* GpuBlockCompressor::add_compression_task (src/block_compressor.rs:342-387).
+ * src_dev: device pointer to row 0 of the source texture (RGBA8 for all
+ *   variants but BC6H, RGBA16F for BC6H); src_pitch: bytes per texture row;
+ *   src_len: bytes of the source allocation reachable from src_dev.
+ * width/height: size of the region to compress; texture_y_offset: first
+ *   texture row of the region (the reference's Option<u32>, 0 = None).
+ * dst_dev/dst_len: destination buffer; blocks_offset: byte offset of the
+ *   region's first block in it (the reference's Option<u32>, 0 = None; like the
+ *   reference, which addresses the buffer in 4-byte words, the offset is
+ *   rounded down to a multiple of 4).
+ * settings: as for bc_compress_rgba8. The task keeps copies of the settings
+ * and of the pointers (the buffers must stay alive until compress returns
+ * work to the stream and that work completes). */
+int bc_compressor_add_task(bc_compressor* c, int variant, const void* settings,
+                           const void* src_dev, size_t src_pitch, size_t src_len, uint32_t width,
+                           uint32_t height, uint32_t texture_y_offset, void* dst_dev,
+                           size_t dst_len, uint32_t blocks_offset);
+
+/* GpuBlockCompressor::compress (src/block_compressor.rs:540-590): enqueues
+ * every pending task on `stream` as one launch per task and drains the queue. */
+int bc_compressor_compress(bc_compressor* c, void* stream);
+
+/* Number of pending tasks. */
+int bc_compressor_task_count(const bc_compressor* c);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* cudaError_t of the last CUDA failure seen on this thread (0 if none). */
+int bc_last_cuda_error(void);
+/* Library version string, e.g. "bcn-b200 0.1.0 (sm_100a)". */
+const char* bc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BC_CAPI_H */
