@@ -322,6 +322,42 @@ def gpu_bench(args, world, rank, local):
         pg.destroy_process_group()
 
 
+def profile_case(args):
+    """Runs one encoder on a square synthetic texture for profilers (ncu):
+    `--case bc7:512` = BC7 alpha_basic on 512x512. Prints one line of kernel
+    timings; it is not a benchmark line."""
+    import torch
+
+    import block_compression_b200 as bcn
+    from block_compression_b200 import synthetic
+
+    name, size = args.case.split(":")
+    size = int(size)
+    V = bcn.CompressionVariant
+    variants = {"bc1": V.BC1, "bc3": V.BC3, "bc4": V.BC4, "bc5": V.BC5,
+                "bc7": V.BC7(bcn.BC7Settings.alpha_basic()), "bc6h": V.BC6H(bcn.BC6HSettings.basic())}
+    v = variants[name]
+    if name == "bc6h":
+        src = torch.from_numpy(synthetic.config3_hdr(seed=3, size=size).view("int16")).cuda()
+    else:
+        src = torch.from_numpy(synthetic.config2_image(seed=2, size=size)).cuda()
+    dst = torch.zeros(v.blocks_byte_size(size, size), dtype=torch.uint8, device="cuda")
+    times = []
+    for i in range(args.warmup + args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        if name == "bc6h":
+            bcn.encode.compress_rgba16(v, src, dst, size, size, size * 4)
+        else:
+            bcn.encode.compress_rgba8(v, src, dst, size, size, size * 4)
+        b.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(a.elapsed_time(b))
+    ms = sum(times) / max(1, len(times))
+    print(json.dumps({"case": args.case, "ms": ms, "mpx_s": size * size / ms / 1e3}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -329,9 +365,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--case", default=None, help="profiling case VARIANT:SIZE, e.g. bc7:512 (not a bench line)")
     args = ap.parse_args()
     world, rank, local = _dist()
-    if args.impl == "reference":
+    if args.case:
+        profile_case(args)
+    elif args.impl == "reference":
         cpu_reference(args, world, rank)
     else:
         gpu_bench(args, world, rank, local)

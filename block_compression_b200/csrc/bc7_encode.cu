@@ -1,27 +1,29 @@
 // BC7 encoder for sm_100a.
 //
-// Work decomposition. A CTA owns a tile of 32 consecutive 4x4 blocks; lane l
-// of every warp works on block l of the tile, so all 32 lanes of a warp always
-// run the same mode and candidate (no intra-warp divergence apart from the
-// per-block partition lists). The candidate space of the reference search
-// (src/encode/bc7.rs:540-879) is swept by the CTA's warps in phases:
+// Work decomposition. Blocks are processed in tiles of 32 consecutive 4x4
+// blocks; lane l of a warp always works on block l of its tile, so the 32
+// lanes of a warp run the same mode and candidate (no intra-warp divergence
+// apart from the per-block partition lists). The reference's per-block
+// search (src/encode/bc7.rs:540-879) becomes a pipeline of launches, each
+// running one narrow code path (a single fused kernel thrashed the
+// instruction cache: every warp of an SM ran a different mode):
 //
-//   1. load     32 blocks -> shared memory, planar f32 (128-bit coalesced loads)
-//   2. bounds   64 (or 128) PCA split bounds per block, spread over warps
-//   3. top-k    per-block ascending selection of the best partitions (modes 1/3/7)
-//   4. search   every partition candidate of modes 0/2/1/3/7, spread over
-//               warps; each warp keeps a first-minimum per mode, merged in
-//               shared memory (smallest error, then earliest candidate)
-//   5. chains   refinement of each mode's winner, every mode-4/5
-//               rotation/index-swap candidate, and mode 6 -- one chain per warp
-//               item; each chain leaves (error, coded 128-bit block) in a slot
-//   6. select   per block, the reference's sequential "strictly better"
-//               comparisons over the slots in the reference mode order
-//   7. store    one 128-bit store per block
+//   prep     PCA split bounds of the 64 partitions, ascending top-k lists
+//            (modes 1/3/7); argmin keys initialised
+//   search   one launch per mode 0/2/1/3/7; grid (tile, candidate group), a
+//            warp evaluates one partition candidate for 32 blocks; the first
+//            minimum per block is kept with a 64-bit atomicMin on
+//            (error bits << 32 | candidate)
+//   refine   one launch per mode: refinement of each block's winner + coding
+//   mode4/5  rotation / index-swap candidates, one warp per candidate
+//   mode6    one warp per tile
+//   select   the reference's sequential "strictly better" scan over the
+//            per-mode results -> one 128-bit store per block
 //
-// Every per-candidate computation keeps the reference's operation order, so
-// the chosen mode, endpoints and indices are bit-identical to the reference
-// CPU encoder (see bc_common.cuh for the float rules).
+// Blocks are staged in shared memory as planar f32 with 128-bit coalesced
+// loads. Every per-candidate computation keeps the reference's operation
+// order, so the chosen mode, endpoints and indices are bit-identical to the
+// reference CPU encoder (see bc_common.cuh for the float rules).
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -33,7 +35,6 @@ namespace bcn {
 namespace bc7 {
 
 using namespace bptc;
-constexpr int NSLOT = 18;   // 5 mode-0/2/1/3/7 results + 12 mode-4/5 candidates + mode 6
 
 // Mode 4/5 candidate block (bc7.rs:680-696): channel `rot` replaced by alpha
 // (4-channel settings) or by 255 (3-channel settings).
@@ -45,24 +46,6 @@ struct BlkRot {
         if (c == rot) return channels == 4 ? p[(48 + k) * NB] : 255.0f;
         return p[(c * 16 + k) * NB];
     }
-};
-
-struct Smem {
-    float px[64][NB];
-    uint32_t map[128];
-    uint8_t anchors[128];
-    float opaque_err[NB];
-    union {
-        int keys[2][64][NB];                // phase 2-3
-        struct {
-            float err[5][8][NB];            // phase 4 per-warp first minima
-            int cand[5][8][NB];
-        } c;
-    } u;
-    uint8_t list[2][64][NB];                // sorted partitions: [0] modes 1/3, [1] mode 7
-    int winner[5][NB];
-    float slot_err[NSLOT][NB];
-    uint4 slot_data[NSLOT][NB];
 };
 
 // ---- endpoint quantisation (bc7.rs:97-237) ----------------------------------
@@ -431,20 +414,20 @@ BCN_DEV float mode6(const Blk& blk, uint32_t refine, uint4& out) {
     return err;
 }
 
-// ---- the kernel -----------------------------------------------------------------
+// ---- kernels --------------------------------------------------------------------
 
-// Candidate-mode bookkeeping index: 0 mode0, 1 mode2, 2 mode1, 3 mode3, 4 mode7
-// (the reference evaluation order).
+// Candidate-mode index mi: 0 mode0, 1 mode2, 2 mode1, 3 mode3, 4 mode7 (the
+// reference evaluation order, bc7.rs:853-867). Slots: mi for modes 0/2/1/3/7,
+// then the mode-4 candidates, the mode-5 candidates, and mode 6.
 struct Plan {
     int count[5];
-    int total;
-    int k_a, k_b;        // top-k lengths of the bound lists
+    int k_a, k_b;        // top-k lengths of the two bound lists
     bool bounds_a, bounds_b;
     int n45_4, n45_5;    // mode-4 / mode-5 candidate counts
     bool run6;
 };
 
-BCN_DEV Plan make_plan(const BC7SettingsDev& s) {
+static __host__ __device__ Plan make_plan(const BC7SettingsDev& s) {
     Plan p;
     bool ms0 = s.mode_selection[0] != 0, ms1 = s.mode_selection[1] != 0;
     bool run13 = ms1 && (s.fast_skip_threshold_mode1 != 0 || s.fast_skip_threshold_mode3 != 0);
@@ -454,14 +437,15 @@ BCN_DEV Plan make_plan(const BC7SettingsDev& s) {
     p.count[2] = run13 ? (int)s.fast_skip_threshold_mode1 : 0;
     p.count[3] = run13 ? (int)s.fast_skip_threshold_mode3 : 0;
     p.count[4] = run7 ? (int)s.fast_skip_threshold_mode7 : 0;
-    p.total = p.count[0] + p.count[1] + p.count[2] + p.count[3] + p.count[4];
     // Mode 7's bounds use the settings' channel count; with 3 channels they
     // equal the mode 1/3 bounds and one sorted list serves both.
     bool sep7 = run7 && s.channels == 4;
-    int k13 = run13 ? (int)max(s.fast_skip_threshold_mode1, s.fast_skip_threshold_mode3) : 0;
+    int t1 = (int)s.fast_skip_threshold_mode1, t3 = (int)s.fast_skip_threshold_mode3;
+    int k13 = run13 ? (t1 > t3 ? t1 : t3) : 0;
     p.bounds_a = run13 || (run7 && !sep7);
     p.bounds_b = sep7;
-    p.k_a = max(k13, (run7 && !sep7) ? (int)s.fast_skip_threshold_mode7 : 0);
+    int k7 = (run7 && !sep7) ? (int)s.fast_skip_threshold_mode7 : 0;
+    p.k_a = k13 > k7 ? k13 : k7;
     p.k_b = sep7 ? (int)s.fast_skip_threshold_mode7 : 0;
     int nrot = s.mode_selection[2] != 0 ? (int)s.channels - (int)s.mode45_channel0 : 0;
     if (nrot < 0) nrot = 0;
@@ -471,59 +455,73 @@ BCN_DEV Plan make_plan(const BC7SettingsDev& s) {
     return p;
 }
 
-template <int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_encode_kernel(const uint8_t* __restrict__ src, size_t stride, uint32_t bw,
-                                                              uint32_t nblocks, uint8_t* __restrict__ dst,
-                                                              BC7SettingsDev S, bool aligned) {
-    static_assert(NW <= 8, "per-warp minima are sized for 8 warps");
-    __shared__ Smem sm;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile0 = blockIdx.x * NB;
-    const Plan P = make_plan(S);
+// Arguments shared by every kernel of one encode. Scratch arrays are indexed
+// [row * npad + block] so a warp's 32 lanes touch 32 consecutive entries.
+struct Work {
+    const uint8_t* src;
+    size_t stride;
+    uint32_t bw, nblocks, npad;
+    bool aligned;
+    uint8_t* dst;
+    uint8_t* lists;            // [(set * 64 + k) * npad + block]
+    unsigned long long* keys;  // [mi * npad + block]: (error bits << 32) | candidate
+    float* slot_err;           // [slot * npad + block]
+    uint4* slot_data;          // [slot * npad + block]
+    BC7SettingsDev S;
+};
 
-    // 1. load ---------------------------------------------------------------
-    for (int i = threadIdx.x; i < 128; i += blockDim.x) {
-        sm.map[i] = kPartitionMap[i];
-        sm.anchors[i] = kAnchors[i];
-    }
-    for (int t = threadIdx.x; t < NB * 4; t += blockDim.x) {
+// Stages the 32 blocks of `tile` into px (planar f32, lane-strided) with
+// threads tid = 0..nt-1 (128-bit loads: the 4 rows of 32 neighbouring blocks
+// are 4 contiguous 512-byte spans).
+BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, int nt) {
+    for (int t = tid; t < NB * 4; t += nt) {
         int b = t & 31, y = t >> 5;
-        uint32_t gi = tile0 + b;
-        uint32_t w[4] = {0, 0, 0, 0};
-        if (gi < nblocks) {
-            uint32_t by = gi / bw, bx = gi - by * bw;
-            const uint8_t* row = src + (size_t)(by * 4 + y) * stride + (size_t)bx * 16;
-            if (aligned) {
-                uint4 v = __ldg(reinterpret_cast<const uint4*>(row));
-                w[0] = v.x;
-                w[1] = v.y;
-                w[2] = v.z;
-                w[3] = v.w;
+        uint32_t gi = tile * NB + b;
+        uint32_t v[4] = {0, 0, 0, 0};
+        if (gi < w.nblocks) {
+            uint32_t by = gi / w.bw, bx = gi - by * w.bw;
+            const uint8_t* row = w.src + (size_t)(by * 4 + y) * w.stride + (size_t)bx * 16;
+            if (w.aligned) {
+                uint4 q = __ldg(reinterpret_cast<const uint4*>(row));
+                v[0] = q.x;
+                v[1] = q.y;
+                v[2] = q.z;
+                v[3] = q.w;
             } else {
-                for (int j = 0; j < 16; j++) w[j >> 2] |= (uint32_t)row[j] << (8 * (j & 3));
+                for (int j = 0; j < 16; j++) v[j >> 2] |= (uint32_t)row[j] << (8 * (j & 3));
             }
         }
 #pragma unroll
         for (int x = 0; x < 4; x++) {
             int k = y * 4 + x;
-            sm.px[k][b] = (float)(w[x] & 0xFF);
-            sm.px[16 + k][b] = (float)((w[x] >> 8) & 0xFF);
-            sm.px[32 + k][b] = (float)((w[x] >> 16) & 0xFF);
-            sm.px[48 + k][b] = (float)(w[x] >> 24);
+            px[k][b] = (float)(v[x] & 0xFF);
+            px[16 + k][b] = (float)((v[x] >> 8) & 0xFF);
+            px[32 + k][b] = (float)((v[x] >> 16) & 0xFF);
+            px[48 + k][b] = (float)(v[x] >> 24);
         }
     }
-    __syncthreads();
-    const float* pxl = &sm.px[0][lane];
-    const Blk blk{pxl};
-    if (warp == 0) {
-        // compute_opaque_err (bc7.rs:869-879)
-        float e = 0.0f;
-        if (S.channels != 3)
-            for (int k = 0; k < 16; k++) e += sqf(blk(3, k) - 255.0f);
-        sm.opaque_err[lane] = e;
-    }
+}
 
-    // 2. PCA split bounds ----------------------------------------------------
+BCN_DEV float opaque_err(const Blk& blk, uint32_t channels) {
+    // compute_opaque_err (bc7.rs:869-879)
+    float e = 0.0f;
+    if (channels != 3)
+        for (int k = 0; k < 16; k++) e += sqf(blk(3, k) - 255.0f);
+    return e;
+}
+
+// K1: PCA split bounds + ascending top-k partition lists (bc7.rs:622-655,
+// 819-851; common.rs:126-140), and argmin-key initialisation.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
+    __shared__ float px[64][NB];
+    __shared__ int keys[2][64][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    const Blk blk{&px[0][lane]};
     const int na = P.bounds_a ? 64 : 0, nb = P.bounds_b ? 64 : 0;
     if (na + nb > 0) {
         float full_a[15], full_b[15];
@@ -531,215 +529,253 @@ __global__ void __launch_bounds__(NW * 32) bc7_encode_kernel(const uint8_t* __re
         if (nb) stats_masked<4>(blk, 0xFFFFu, full_b);
         for (int item = warp; item < na + nb; item += NW) {
             if (item < na) {
-                int part = item;
-                float b12 = pca_bound_split<3>(blk, subset_mask_from_map(sm.map[part], 0), full_a);
-                sm.u.keys[0][part][lane] = part + (int)b12 * 64;
+                float b12 = pca_bound_split<3>(blk, subset_mask_from_map(kPartitionMap[item], 0), full_a);
+                keys[0][item][lane] = item + (int)b12 * 64;
             } else {
                 int part = item - na;
-                float b12 = pca_bound_split<4>(blk, subset_mask_from_map(sm.map[part], 0), full_b);
-                sm.u.keys[1][part][lane] = part + (int)b12 * 64;
+                float b12 = pca_bound_split<4>(blk, subset_mask_from_map(kPartitionMap[part], 0), full_b);
+                keys[1][part][lane] = part + (int)b12 * 64;
             }
         }
     }
     __syncthreads();
-
-    // 3. top-k (partial_sort_list, common.rs:126-140: ascending, keys unique) --
+    // partial_sort_list: keys are unique, so the first K entries are the K
+    // smallest in ascending order.
     for (int set = 0; set < 2; set++) {
         int K = set == 0 ? P.k_a : P.k_b;
-        if (K == 0 || warp != (set % NW)) continue;
+        if (K == 0 || warp != set) continue;
         for (int k = 0; k < K; k++) {
             int best = INT_MAX, bi = 0;
             for (int q = 0; q < 64; q++) {
-                int v = sm.u.keys[set][q][lane];
+                int v = keys[set][q][lane];
                 if (v < best) {
                     best = v;
                     bi = q;
                 }
             }
-            sm.list[set][k][lane] = (uint8_t)bi;
-            sm.u.keys[set][bi][lane] = INT_MAX;
+            keys[set][bi][lane] = INT_MAX;
+            w.lists[(size_t)(set * 64 + k) * w.npad + gi] = (uint8_t)bi;
         }
     }
-    __syncthreads();
+    if (warp == NW - 1)
+        for (int m = 0; m < 5; m++) w.keys[(size_t)m * w.npad + gi] = ~0ull;
+}
 
-    // 4. partition candidates of modes 0/2/1/3/7 ----------------------------------
-    {
-        float berr[5];
-        int bcand[5];
-#pragma unroll
-        for (int m = 0; m < 5; m++) {
-            berr[m] = __int_as_float(0x7f800000);
-            bcand[m] = -1;
-        }
-        const int list7 = P.bounds_b ? 1 : 0;
-        for (int item = warp; item < P.total; item += NW) {
-            int mi = 0, ci = item;
-            while (ci >= P.count[mi]) {
-                ci -= P.count[mi];
-                mi++;
-            }
-            int qep[24];
-            uint32_t q0, q1;
-            float err;
-            switch (mi) {
-                case 0: err = eval_part<0>(blk, sm.map, ci + 64, qep, q0, q1); break;
-                case 1: err = eval_part<2>(blk, sm.map, ci + 64, qep, q0, q1); break;
-                case 2: err = eval_part<1>(blk, sm.map, sm.list[0][ci][lane], qep, q0, q1); break;
-                case 3: err = eval_part<3>(blk, sm.map, sm.list[0][ci][lane], qep, q0, q1); break;
-                default: err = eval_part<7>(blk, sm.map, sm.list[list7][ci][lane], qep, q0, q1); break;
-            }
-#pragma unroll
-            for (int m = 0; m < 5; m++)
-                if (m == mi && err < berr[m]) {
-                    berr[m] = err;
-                    bcand[m] = ci;
-                }
-        }
-#pragma unroll
-        for (int m = 0; m < 5; m++) {
-            sm.u.c.err[m][warp][lane] = berr[m];
-            sm.u.c.cand[m][warp][lane] = bcand[m];
-        }
+BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
+    if (mi <= 1) return c + 64;  // modes 0 and 2: partitions 0..count-1 of the 3-subset table
+    int set = (mi == 4 && P.bounds_b) ? 1 : 0;
+    return w.lists[(size_t)(set * 64 + c) * w.npad + gi];
+}
+
+// K2: every partition candidate of one mode (bc7.rs:517-569). Grid: (tile,
+// candidate group); warp w evaluates candidate blockIdx.y*NW+w for the 32
+// blocks of the tile. The CTA's first minimum per block goes to the global
+// argmin key with a 64-bit atomicMin -- errors are non-negative, so their bit
+// patterns order like the values, and the low word breaks ties toward the
+// earlier candidate, exactly the reference's strict "<" scan.
+template <int MODE, int NW>
+__global__ void __launch_bounds__(NW * 32) bc7_search_kernel(Work w) {
+    constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
+    __shared__ float px[64][NB];
+    __shared__ unsigned long long best[NW][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    const int c = blockIdx.y * NW + warp;
+    unsigned long long key = ~0ull;
+    if (c < P.count[mi] && gi < w.nblocks) {
+        const Blk blk{&px[0][lane]};
+        int qep[24];
+        uint32_t q0, q1;
+        float err = eval_part<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1);
+        if (err == err) key = ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c;
     }
+    best[warp][lane] = key;
     __syncthreads();
     if (warp == 0) {
-        for (int m = 0; m < 5; m++) {
-            float be = __int_as_float(0x7f800000);
-            int bc = -1;
-            for (int w = 0; w < NW; w++) {
-                float e = sm.u.c.err[m][w][lane];
-                int c = sm.u.c.cand[m][w][lane];
-                if (c >= 0 && (bc < 0 || e < be || (e == be && c < bc))) {
-                    be = e;
-                    bc = c;
-                }
-            }
-            sm.winner[m][lane] = bc;
-            sm.slot_err[m][lane] = be;  // unrefined error of the winner (phase 5 input)
-        }
+        unsigned long long k = best[0][lane];
+        for (int i = 1; i < NW; i++) k = min(k, best[i][lane]);
+        if (k != ~0ull) atomicMin(&w.keys[(size_t)mi * w.npad + gi], k);
     }
-    __syncthreads();
+}
 
-    // 5. chains: refinements, mode 4/5 candidates, mode 6 -------------------------
-    {
-        const int n_ref = 5, n45 = P.n45_4 + P.n45_5, n_items = n_ref + n45 + 1;
-        const int list7 = P.bounds_b ? 1 : 0;
-        for (int item = warp; item < n_items; item += NW) {
-            float err = __int_as_float(0x7f800000);
-            uint4 data = make_uint4(0, 0, 0, 0);
-            if (item < n_ref) {
-                int mi = item;
-                int wc = sm.winner[mi][lane];
-                float e0 = sm.slot_err[mi][lane];
-                if (P.count[mi] > 0 && wc >= 0) {
-                    float oe = sm.opaque_err[lane];
-                    switch (mi) {
-                        case 0: err = refine_and_code<0>(blk, sm.map, wc + 64, e0, S.refine_iterations[0], oe, data); break;
-                        case 1: err = refine_and_code<2>(blk, sm.map, wc + 64, e0, S.refine_iterations[2], oe, data); break;
-                        case 2:
-                            err = refine_and_code<1>(blk, sm.map, sm.list[0][wc][lane], e0, S.refine_iterations[1], oe, data);
-                            break;
-                        case 3:
-                            err = refine_and_code<3>(blk, sm.map, sm.list[0][wc][lane], e0, S.refine_iterations[3], oe, data);
-                            break;
-                        default:
-                            err = refine_and_code<7>(blk, sm.map, sm.list[list7][wc][lane], e0, S.refine_iterations[7], oe,
-                                                     data);
-                            break;
-                    }
-                }
-            } else if (item < n_ref + n45) {
-                int c = item - n_ref;
-                if (c < P.n45_4) {
-                    int rot = (int)S.mode45_channel0 + c / 2, swap = c & 1;
-                    err = mode45_candidate<4>(pxl, (int)S.channels, S.refine_iterations[4], S.refine_iterations_channel,
-                                              rot, swap, data);
-                } else {
-                    int rot = (int)S.mode45_channel0 + (c - P.n45_4);
-                    err = mode45_candidate<5>(pxl, (int)S.channels, S.refine_iterations[5], S.refine_iterations_channel,
-                                              rot, 0, data);
-                }
-            } else if (P.run6) {
-                if (S.channels == 3) err = mode6<3>(blk, S.refine_iterations[6], data);
-                else err = mode6<4>(blk, S.refine_iterations[6], data);
-            }
-            // Refinement items overwrite the unrefined error phase 4 left in
-            // their own slot; no other warp reads that slot.
-            sm.slot_err[item][lane] = err;
-            sm.slot_data[item][lane] = data;
-        }
+// K3: refinement of each block's winning partition + coding (bc7.rs:571-609).
+// One warp per tile.
+template <int MODE, int NW>
+__global__ void __launch_bounds__(NW * 32) bc7_refine_kernel(Work w, uint32_t ntiles) {
+    constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
+    __shared__ float px[NW][64][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x * NW + warp;
+    if (tile >= ntiles) return;
+    stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    const uint32_t gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    const Blk blk{&px[warp][0][lane]};
+    unsigned long long key = w.keys[(size_t)mi * w.npad + gi];
+    float err = __int_as_float(0x7f800000);
+    uint4 data = make_uint4(0, 0, 0, 0);
+    if (key != ~0ull && gi < w.nblocks) {
+        int c = (int)(key & 0xFFFFFFFFu);
+        float e0 = __uint_as_float((uint32_t)(key >> 32));
+        int iters = (int)w.S.refine_iterations[MODE];
+        err = refine_and_code<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), e0, iters,
+                                    opaque_err(blk, w.S.channels), data);
     }
-    __syncthreads();
+    w.slot_err[(size_t)mi * w.npad + gi] = err;
+    w.slot_data[(size_t)mi * w.npad + gi] = data;
+}
 
-    // 6. select (the reference's sequential strict comparisons) --------------------
-    if (warp == 0) {
-        float best = __int_as_float(0x7f800000);
-        uint4 data = make_uint4(0, 0, 0, 0);
-        for (int s = 0; s < 5; s++) {
-            float e = sm.slot_err[s][lane];
+// K4: mode 4 / mode 5 rotation (and, for mode 4, index-swap) candidates
+// (bc7.rs:657-760). Grid: (tile, candidate group), warp = candidate.
+template <int MODE, int NW>
+__global__ void __launch_bounds__(NW * 32) bc7_mode45_kernel(Work w) {
+    __shared__ float px[64][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    const int c = blockIdx.y * NW + warp;
+    const int n = MODE == 4 ? P.n45_4 : P.n45_5;
+    if (c >= n) return;
+    int rot = MODE == 4 ? (int)w.S.mode45_channel0 + c / 2 : (int)w.S.mode45_channel0 + c;
+    int swap = MODE == 4 ? (c & 1) : 0;
+    uint4 data;
+    float err = mode45_candidate<MODE>(&px[0][lane], (int)w.S.channels, w.S.refine_iterations[MODE],
+                                       w.S.refine_iterations_channel, rot, swap, data);
+    int slot = 5 + (MODE == 4 ? c : P.n45_4 + c);
+    w.slot_err[(size_t)slot * w.npad + gi] = err;
+    w.slot_data[(size_t)slot * w.npad + gi] = data;
+}
+
+// K5: mode 6 (bc7.rs:762-817), one warp per tile.
+template <int CH, int NW>
+__global__ void __launch_bounds__(NW * 32) bc7_mode6_kernel(Work w, uint32_t ntiles) {
+    __shared__ float px[NW][64][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x * NW + warp;
+    if (tile >= ntiles) return;
+    stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    const Plan P = make_plan(w.S);
+    const uint32_t gi = tile * NB + lane;
+    const Blk blk{&px[warp][0][lane]};
+    uint4 data;
+    float err = mode6<CH>(blk, w.S.refine_iterations[6], data);
+    int slot = 5 + P.n45_4 + P.n45_5;
+    w.slot_err[(size_t)slot * w.npad + gi] = err;
+    w.slot_data[(size_t)slot * w.npad + gi] = data;
+}
+
+// K6: the reference keeps a candidate only when its error is strictly below
+// the best so far, scanning modes 0,2,1,3,7, the mode-4 then mode-5
+// candidates, then mode 6 (bc7.rs:602-609, 735-760, 813-816): the first slot
+// holding the minimum wins. A block no mode encodes stays all-zero.
+__global__ void __launch_bounds__(256) bc7_select_kernel(Work w) {
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= w.nblocks) return;
+    const Plan P = make_plan(w.S);
+    float best = __int_as_float(0x7f800000);
+    int win = -1;
+    for (int s = 0; s < 5; s++)
+        if (P.count[s] > 0) {
+            float e = w.slot_err[(size_t)s * w.npad + gi];
             if (e < best) {
                 best = e;
-                data = sm.slot_data[s][lane];
+                win = s;
             }
         }
-        const int b45 = 5;
-        float be = best;
-        int cand = -1;
-        for (int c = 0; c < P.n45_4; c++) {
-            float e = sm.slot_err[b45 + c][lane];
-            if (e < be) {
-                be = e;
-                cand = b45 + c;
-            }
+    const int n45 = P.n45_4 + P.n45_5;
+    for (int s = 5; s < 5 + n45; s++) {
+        float e = w.slot_err[(size_t)s * w.npad + gi];
+        if (e < best) {
+            best = e;
+            win = s;
         }
-        if (be < best) {
-            best = be;
-            data = sm.slot_data[cand][lane];
+    }
+    if (P.run6) {
+        int s = 5 + n45;
+        float e = w.slot_err[(size_t)s * w.npad + gi];
+        if (e < best) {
+            best = e;
+            win = s;
         }
-        for (int c = 0; c < P.n45_5; c++) {
-            float e = sm.slot_err[b45 + P.n45_4 + c][lane];
-            if (e < be) {
-                be = e;
-                cand = b45 + P.n45_4 + c;
-            }
-        }
-        if (be < best) {
-            best = be;
-            data = sm.slot_data[cand][lane];
-        }
-        int s6 = b45 + P.n45_4 + P.n45_5;
-        float e6 = sm.slot_err[s6][lane];
-        if (P.run6 && e6 < best) {
-            best = e6;
-            data = sm.slot_data[s6][lane];
-        }
-        // 7. store
-        uint32_t gi = tile0 + lane;
-        if (gi < nblocks) {
-            uint8_t* o = dst + (size_t)gi * 16;
-            if (((uintptr_t)dst & 15) == 0) {
-                *reinterpret_cast<uint4*>(o) = data;
-            } else {
-                uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
-                o32[0] = data.x;
-                o32[1] = data.y;
-                o32[2] = data.z;
-                o32[3] = data.w;
-            }
-        }
+    }
+    uint4 data = win >= 0 ? w.slot_data[(size_t)win * w.npad + gi] : make_uint4(0, 0, 0, 0);
+    uint8_t* o = w.dst + (size_t)gi * 16;
+    if (((uintptr_t)w.dst & 15) == 0) {
+        *reinterpret_cast<uint4*>(o) = data;
+    } else {
+        uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+        o32[0] = data.x;
+        o32[1] = data.y;
+        o32[2] = data.z;
+        o32[3] = data.w;
     }
 }
 
 }  // namespace bc7
 
-void launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
-                       const BC7SettingsDev& settings, cudaStream_t s) {
+size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& s) {
+    const bc7::Plan P = bc7::make_plan(s);
+    size_t npad = ((size_t)nblocks + bc7::NB - 1) / bc7::NB * bc7::NB;
+    int nslots = 5 + P.n45_4 + P.n45_5 + 1;
+    return npad * (128 + 5 * 8 + (size_t)nslots * (4 + 16)) + 256;
+}
+
+cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s) {
+    using namespace bc7;
     uint32_t n = bw * bh;
-    if (n == 0) return;
-    constexpr int NW = 4;
-    bool aligned = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
-    uint32_t grid = (n + bc7::NB - 1) / bc7::NB;
-    bc7::bc7_encode_kernel<NW><<<grid, NW * 32, 0, s>>>(src, stride, bw, n, dst, settings, aligned);
+    if (n == 0) return cudaSuccess;
+    const Plan P = make_plan(settings);
+    uint32_t ntiles = (n + NB - 1) / NB;
+    size_t npad = (size_t)ntiles * NB;
+    int nslots = 5 + P.n45_4 + P.n45_5 + 1;
+    Work w;
+    w.src = src;
+    w.stride = stride;
+    w.bw = bw;
+    w.nblocks = n;
+    w.npad = (uint32_t)npad;
+    w.aligned = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
+    w.dst = dst;
+    uint8_t* p = (uint8_t*)(((uintptr_t)scratch + 255) & ~(uintptr_t)255);
+    w.slot_data = (uint4*)p;
+    p += npad * 16 * nslots;
+    w.keys = (unsigned long long*)p;
+    p += npad * 8 * 5;
+    w.slot_err = (float*)p;
+    p += npad * 4 * nslots;
+    w.lists = p;
+    w.S = settings;
+
+    constexpr int NWP = 8, NWS = 8, NWR = 4, NW45 = 4;
+    bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
+    auto groups = [](int count, int nw) { return (unsigned)((count + nw - 1) / nw); };
+    if (P.count[0]) bc7_search_kernel<0, NWS><<<dim3(ntiles, groups(P.count[0], NWS)), NWS * 32, 0, s>>>(w);
+    if (P.count[1]) bc7_search_kernel<2, NWS><<<dim3(ntiles, groups(P.count[1], NWS)), NWS * 32, 0, s>>>(w);
+    if (P.count[2]) bc7_search_kernel<1, NWS><<<dim3(ntiles, groups(P.count[2], NWS)), NWS * 32, 0, s>>>(w);
+    if (P.count[3]) bc7_search_kernel<3, NWS><<<dim3(ntiles, groups(P.count[3], NWS)), NWS * 32, 0, s>>>(w);
+    if (P.count[4]) bc7_search_kernel<7, NWS><<<dim3(ntiles, groups(P.count[4], NWS)), NWS * 32, 0, s>>>(w);
+    unsigned rgrid = (ntiles + NWR - 1) / NWR;
+    if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (P.n45_4) bc7_mode45_kernel<4, NW45><<<dim3(ntiles, groups(P.n45_4, NW45)), NW45 * 32, 0, s>>>(w);
+    if (P.n45_5) bc7_mode45_kernel<5, NW45><<<dim3(ntiles, groups(P.n45_5, NW45)), NW45 * 32, 0, s>>>(w);
+    if (P.run6) {
+        if (settings.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+        else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    }
+    bc7_select_kernel<<<(n + 255) / 256, 256, 0, s>>>(w);
+    return cudaGetLastError();
 }
 
 }  // namespace bcn

@@ -30,8 +30,11 @@ void launch_bc15_encode(int variant, const uint8_t* src, size_t stride, uint32_t
                         cudaStream_t s);
 void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch,
                         cudaStream_t s);
-void launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
-                       const BC7SettingsDev& settings, cudaStream_t s);
+// BC7 runs as a short pipeline of kernels that exchange per-block state
+// through `scratch` (device memory of at least bc7_scratch_bytes()).
+size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& settings);
+cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s);
 void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s);
 // stride in bytes of the source rows (RGBA16F: 8 bytes per pixel; RGBA8: 4).
 void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,

@@ -67,9 +67,18 @@ static int enqueue_encode(int variant, const void* settings, const uint8_t* src,
     uint32_t bw = (w + 3) / 4, bh = (h + 3) / 4;
     if (bw == 0 || bh == 0) return BC_OK;
     switch (variant) {
-        case BC_BC7:
-            launch_bc7_encode(src, stride, bw, bh, dst, *(const BC7SettingsDev*)settings, s);
+        case BC_BC7: {
+            // Stream-ordered scratch from the device's default memory pool:
+            // freed (returned to the pool) once the launches have run.
+            const BC7SettingsDev& s7 = *(const BC7SettingsDev*)settings;
+            void* scratch = nullptr;
+            BC_CUDA(cudaMallocAsync(&scratch, bc7_scratch_bytes(bw * bh, s7), s));
+            cudaError_t e = launch_bc7_encode(src, stride, bw, bh, dst, s7, scratch, s);
+            cudaError_t f = cudaFreeAsync(scratch, s);
+            BC_CUDA(e);
+            BC_CUDA(f);
             break;
+        }
         case BC_BC6H: {
             int rc = upload_bc6h_tables();
             if (rc != BC_OK) return rc;
