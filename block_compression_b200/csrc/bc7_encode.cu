@@ -38,12 +38,12 @@ using namespace bptc;
 
 // Mode 4/5 candidate block (bc7.rs:680-696): channel `rot` replaced by alpha
 // (4-channel settings) or by 255 (3-channel settings).
+template <bool CH4>
 struct BlkRot {
     const float* p;
     int rot;
-    int channels;
     BCN_DEV float operator()(int c, int k) const {
-        if (c == rot) return channels == 4 ? p[(48 + k) * NB] : 255.0f;
+        if (c == rot) return CH4 ? p[(48 + k) * NB] : 255.0f;
         return p[(c * 16 + k) * NB];
     }
 };
@@ -293,17 +293,17 @@ BCN_DEV void channel_opt_endpoints(float ep[2], const float cb[16], int bits, ui
     }
 }
 
-// One mode-4/5 candidate: rotation `rot`, index swap `swap`. Returns its
-// error and its coded block (bc7_code_mode45 for MODE).
-template <int MODE>
-BCN_DEV float mode45_candidate(const float* pxlane, int channels, uint32_t refine, uint32_t refine_channel, int rot,
-                               int swap, uint4& out) {
-    int bits = 2, abits = MODE == 4 ? 3 : 2, aepbits = MODE == 4 ? 6 : 8;
-    if (swap == 1) {
-        bits = 3;
-        abits = 2;
-    }
-    BlkRot cb{pxlane, rot < 3 ? rot : -1, channels};
+// One mode-4/5 candidate: rotation `rot`, index swap SWAP (mode 4 only),
+// CH4 = 4-channel settings. Returns its error and its coded block
+// (bc7_code_mode45 for MODE). The index widths are compile-time so that one
+// launch runs a single instruction stream.
+template <int MODE, int SWAP, bool CH4>
+BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t refine_channel, int rot, uint4& out) {
+    constexpr int bits = SWAP ? 3 : 2;
+    constexpr int abits = SWAP ? 2 : (MODE == 4 ? 3 : 2);
+    constexpr int aepbits = MODE == 4 ? 6 : 8;
+    const int swap = SWAP;
+    BlkRot<CH4> cb{pxlane, rot < 3 ? rot : -1};
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     block_segment<3, true>(cb, 0xFFFFu, ep);
     int qep[8];
@@ -312,14 +312,13 @@ BCN_DEV float mode45_candidate(const float* pxlane, int channels, uint32_t refin
 #pragma unroll
     for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
     uint32_t q0, q1;
-    float err = bits == 2 ? block_quant<3, 2, 1>(cb, ep, 0, q0, q1) : block_quant<3, 3, 1>(cb, ep, 0, q0, q1);
+    float err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
     for (uint32_t it = 0; it < refine; it++) {
-        if (bits == 2) opt_endpoints<3, 2>(ep, cb, q0, q1, 0xFFFFu);
-        else opt_endpoints<3, 3>(ep, cb, q0, q1, 0xFFFFu);
+        opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
         quant245<EPB, 8>(qep, ep);
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
-        err = bits == 2 ? block_quant<3, 2, 1>(cb, ep, 0, q0, q1) : block_quant<3, 3, 1>(cb, ep, 0, q0, q1);
+        err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
     float chan[16];
@@ -463,7 +462,7 @@ struct Work {
     uint32_t bw, nblocks, npad;
     bool aligned;
     uint8_t* dst;
-    uint8_t* lists;            // [(set * 64 + k) * npad + block]
+    uint8_t* lists;            // [row * npad + block]: rows 0..k_a-1 list A, then k_b rows of list B
     unsigned long long* keys;  // [mi * npad + block]: (error bits << 32) | candidate
     float* slot_err;           // [slot * npad + block]
     uint4* slot_data;          // [slot * npad + block]
@@ -554,7 +553,7 @@ __global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
                 }
             }
             keys[set][bi][lane] = INT_MAX;
-            w.lists[(size_t)(set * 64 + k) * w.npad + gi] = (uint8_t)bi;
+            w.lists[(size_t)(set == 0 ? k : P.k_a + k) * w.npad + gi] = (uint8_t)bi;
         }
     }
     if (warp == NW - 1)
@@ -563,8 +562,8 @@ __global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
 
 BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
     if (mi <= 1) return c + 64;  // modes 0 and 2: partitions 0..count-1 of the 3-subset table
-    int set = (mi == 4 && P.bounds_b) ? 1 : 0;
-    return w.lists[(size_t)(set * 64 + c) * w.npad + gi];
+    int row = (mi == 4 && P.bounds_b) ? P.k_a + c : c;
+    return w.lists[(size_t)row * w.npad + gi];
 }
 
 // K2: every partition candidate of one mode (bc7.rs:517-569). Grid: (tile,
@@ -629,9 +628,10 @@ __global__ void __launch_bounds__(NW * 32) bc7_refine_kernel(Work w, uint32_t nt
     w.slot_data[(size_t)mi * w.npad + gi] = data;
 }
 
-// K4: mode 4 / mode 5 rotation (and, for mode 4, index-swap) candidates
-// (bc7.rs:657-760). Grid: (tile, candidate group), warp = candidate.
-template <int MODE, int NW>
+// K4: mode 4 / mode 5 rotation candidates (bc7.rs:657-760); mode 4 runs one
+// launch per index-swap setting. Grid: (tile, rotation group), warp = one
+// rotation for the tile's 32 blocks.
+template <int MODE, int SWAP, bool CH4, int NW>
 __global__ void __launch_bounds__(NW * 32) bc7_mode45_kernel(Work w) {
     __shared__ float px[64][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -639,15 +639,15 @@ __global__ void __launch_bounds__(NW * 32) bc7_mode45_kernel(Work w) {
     const Plan P = make_plan(w.S);
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
-    const int c = blockIdx.y * NW + warp;
-    const int n = MODE == 4 ? P.n45_4 : P.n45_5;
-    if (c >= n) return;
-    int rot = MODE == 4 ? (int)w.S.mode45_channel0 + c / 2 : (int)w.S.mode45_channel0 + c;
-    int swap = MODE == 4 ? (c & 1) : 0;
+    const int r = blockIdx.y * NW + warp;  // rotation index
+    if (r >= P.n45_5) return;              // n45_5 = number of rotations
+    int rot = (int)w.S.mode45_channel0 + r;
     uint4 data;
-    float err = mode45_candidate<MODE>(&px[0][lane], (int)w.S.channels, w.S.refine_iterations[MODE],
-                                       w.S.refine_iterations_channel, rot, swap, data);
-    int slot = 5 + (MODE == 4 ? c : P.n45_4 + c);
+    float err = mode45_candidate<MODE, SWAP, CH4>(&px[0][lane], w.S.refine_iterations[MODE],
+                                                  w.S.refine_iterations_channel, rot, data);
+    // candidate order of the reference: mode 4 (rotation, swap 0), (rotation,
+    // swap 1), ... then mode 5 rotations
+    int slot = 5 + (MODE == 4 ? 2 * r + SWAP : P.n45_4 + r);
     w.slot_err[(size_t)slot * w.npad + gi] = err;
     w.slot_data[(size_t)slot * w.npad + gi] = data;
 }
@@ -724,7 +724,7 @@ size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& s) {
     const bc7::Plan P = bc7::make_plan(s);
     size_t npad = ((size_t)nblocks + bc7::NB - 1) / bc7::NB * bc7::NB;
     int nslots = 5 + P.n45_4 + P.n45_5 + 1;
-    return npad * (128 + 5 * 8 + (size_t)nslots * (4 + 16)) + 256;
+    return npad * ((size_t)(P.k_a + P.k_b) + 5 * 8 + (size_t)nslots * (4 + 16)) + 256;
 }
 
 cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
@@ -768,8 +768,18 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
     if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (P.n45_4) bc7_mode45_kernel<4, NW45><<<dim3(ntiles, groups(P.n45_4, NW45)), NW45 * 32, 0, s>>>(w);
-    if (P.n45_5) bc7_mode45_kernel<5, NW45><<<dim3(ntiles, groups(P.n45_5, NW45)), NW45 * 32, 0, s>>>(w);
+    if (P.n45_5) {
+        dim3 g45(ntiles, groups(P.n45_5, NW45));
+        if (settings.channels == 4) {
+            bc7_mode45_kernel<4, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+            bc7_mode45_kernel<4, 1, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+            bc7_mode45_kernel<5, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+        } else {
+            bc7_mode45_kernel<4, 0, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+            bc7_mode45_kernel<4, 1, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+            bc7_mode45_kernel<5, 0, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
+        }
+    }
     if (P.run6) {
         if (settings.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
         else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);

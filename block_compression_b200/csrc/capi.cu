@@ -60,6 +60,35 @@ static int check_settings(int variant, const void* settings) {
     return BC_OK;
 }
 
+// Per-device memory pool for the stream-ordered scratch of multi-kernel
+// encodes. Its release threshold is unlimited, so memory freed at the end of
+// one call is reused by the next instead of being unmapped at every
+// synchronisation (the default pool's threshold is 0). The pool belongs to
+// this library; the caller's default pool is left untouched.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64];
+
+static int scratch_pool(cudaMemPool_t* out) {
+    int dev = 0;
+    BC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return BC_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        BC_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t threshold = UINT64_MAX;
+        BC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return BC_OK;
+}
+
 // Enqueues the encode of a w x h region whose row 0 is at `src`.
 // bytes_per_px: 4 (RGBA8) or 8 (RGBA16F, BC6H only).
 static int enqueue_encode(int variant, const void* settings, const uint8_t* src, size_t stride, uint32_t w,
@@ -68,11 +97,14 @@ static int enqueue_encode(int variant, const void* settings, const uint8_t* src,
     if (bw == 0 || bh == 0) return BC_OK;
     switch (variant) {
         case BC_BC7: {
-            // Stream-ordered scratch from the device's default memory pool:
-            // freed (returned to the pool) once the launches have run.
+            // Stream-ordered scratch from the library's pool: returned to the
+            // pool once the launches have run.
             const BC7SettingsDev& s7 = *(const BC7SettingsDev*)settings;
+            cudaMemPool_t pool;
+            int prc = scratch_pool(&pool);
+            if (prc != BC_OK) return prc;
             void* scratch = nullptr;
-            BC_CUDA(cudaMallocAsync(&scratch, bc7_scratch_bytes(bw * bh, s7), s));
+            BC_CUDA(cudaMallocFromPoolAsync(&scratch, bc7_scratch_bytes(bw * bh, s7), pool, s));
             cudaError_t e = launch_bc7_encode(src, stride, bw, bh, dst, s7, scratch, s);
             cudaError_t f = cudaFreeAsync(scratch, s);
             BC_CUDA(e);
