@@ -6,6 +6,12 @@
 // path against the reference algorithm. Nothing in the shipped library links
 // or calls this code.
 //
+// Pinning: the decoders are pinned by the reference's 18 decoder known-answer
+// tests (tests/golden/decoder_kat.json); the encoders are parity unpinned --
+// the reference ships no encode golden vectors and cannot be built here (no
+// Rust toolchain), so the encoder half rests on transcription fidelity plus
+// round trips through the pinned decoders.
+//
 // Floating point rules that keep it bit-identical to the Rust source:
 //   * built with -O2 -ffp-contract=off (no FMA contraction), no fast-math;
 //   * every f32 operation is written in the Rust source order;
