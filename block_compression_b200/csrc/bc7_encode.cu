@@ -789,3 +789,77 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
 }
 
 }  // namespace bcn
+
+// ---- allocation-free BC7 entry point ---------------------------------------------
+//
+// bc_compress_bc7_device_noalloc runs the same kernels as the regular entry
+// point, with their scratch in the fixed array below instead of memory
+// allocated per call, for callers that may not allocate device memory during
+// the call (see include/bc_capi.h).
+
+#include <mutex>
+
+#include "../../include/bc_capi.h"
+
+namespace bcn {
+namespace {
+
+static __device__ __align__(256) uint8_t g_bc7_noalloc_scratch[BC_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64];  // device address of the array, per device ordinal
+
+// Device address of the array on the current device. The array's name in host
+// code is only a host-side handle; the kernels need the address the runtime
+// reports for the current device, looked up once per device.
+int noalloc_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return BC_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 64) return BC_ERR_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_bc7_noalloc_scratch);
+        if (e != cudaSuccess) {
+            record_cuda_error(e);
+            return BC_ERR_CUDA;
+        }
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return BC_OK;
+}
+
+}  // namespace
+}  // namespace bcn
+
+extern "C" int bc_compress_bc7_device_noalloc(const bc_bc7_settings* settings, const uint8_t* rgba_dev,
+                                              size_t rgba_len, uint8_t* blocks_dev, size_t blocks_len,
+                                              uint32_t width, uint32_t height, size_t stride_bytes, void* stream) {
+    using namespace bcn;
+    // The checks of bc_compress_rgba8_device (src/encode.rs:91-101).
+    if (height % 4 != 0 || width % 4 != 0) return BC_ERR_DIMS;
+    int rc = validate_bc7_settings(settings);
+    if (rc != BC_OK) return rc;
+    uint32_t bw = width / 4, bh = height / 4;
+    if (blocks_len < (size_t)bw * bh * 16) return BC_ERR_DST_SIZE;
+    if (width > 0 && height > 0 && rgba_len < (size_t)(height - 1) * stride_bytes + (size_t)width * 4)
+        return BC_ERR_SRC_SIZE;
+    if (width == 0 || height == 0) return BC_OK;
+    if (!rgba_dev || !blocks_dev) return BC_ERR_NULL;
+    const BC7SettingsDev& s7 = *reinterpret_cast<const BC7SettingsDev*>(settings);
+    if (bc7_scratch_bytes(bw * bh, s7) > BC_NOALLOC_SCRATCH_BYTES) return BC_ERR_TOO_LARGE;
+    void* scratch = nullptr;
+    rc = noalloc_scratch_address(&scratch);
+    if (rc != BC_OK) return rc;
+    cudaError_t e = launch_bc7_encode(rgba_dev, stride_bytes, bw, bh, blocks_dev, s7, scratch, (cudaStream_t)stream);
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return BC_ERR_CUDA;
+    }
+    return BC_OK;
+}

@@ -44,6 +44,11 @@ void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format,
 void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
                         cudaStream_t s);
 
+// Settings check shared by every BC7 entry point (BC_OK or a BC_ERR_* code),
+// and the per-thread record behind bc_last_cuda_error().
+int validate_bc7_settings(const void* settings);
+void record_cuda_error(cudaError_t e);
+
 // One-time per-device table upload (sRGB conversion LUTs computed on the host).
 int upload_bc6h_tables();
 // Copies a host table into the device symbol of the translation unit that

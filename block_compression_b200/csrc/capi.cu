@@ -53,6 +53,10 @@ static int check_bc6h(const void* p) {
     return BC_OK;
 }
 
+// Entry points defined in other translation units share these checks.
+int validate_bc7_settings(const void* p) { return check_bc7(p); }
+void record_cuda_error(cudaError_t e) { t_last_cuda_error = (int)e; }
+
 static int check_settings(int variant, const void* settings) {
     if (variant < 0 || variant > 6) return BC_ERR_VARIANT;
     if (variant == BC_BC7) return check_bc7(settings);

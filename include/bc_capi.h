@@ -107,6 +107,36 @@ int bc_compress_rgba16_device(const bc_bc6h_settings* settings, const uint16_t* 
                               size_t rgba_len, uint8_t* blocks_dev, size_t blocks_len,
                               uint32_t width, uint32_t height, size_t stride_elems, void* stream);
 
+/* ---- encode without allocating ---------------------------------------------
+ * No counterpart in the reference. BC7 encode of device buffers exactly like
+ * bc_compress_rgba8_device (same bytes), except that it allocates nothing:
+ * the per-block scratch the BC7 kernels exchange lives in a fixed device
+ * array compiled into the library (BC_NOALLOC_SCRATCH_BYTES, held on every
+ * GPU that loads the library until the process exits).
+ *
+ * For callers that must not allocate device memory inside the call: engines
+ * and plugins that own every byte of GPU memory through their own budgeted
+ * allocator, code on a frame-critical thread that cannot risk an allocator
+ * lock or an out-of-memory failure mid-frame, and processes running with the
+ * device nearly full.
+ *
+ * Limits and rules:
+ *  - images whose scratch need exceeds BC_NOALLOC_SCRATCH_BYTES are rejected
+ *    with BC_ERR_TOO_LARGE; every preset fits images up to 1024x1024 pixels;
+ *  - the first call on a device looks up the array's device address (a
+ *    one-time set-up per device); make that first call before any stream
+ *    capture;
+ *  - all calls share the one array and it keeps the last call's contents:
+ *    calls that overlap on the GPU (other streams, other host threads) race
+ *    and corrupt each other's results; serialise them.
+ */
+#define BC_NOALLOC_SCRATCH_BYTES (40u * 1024u * 1024u)
+#define BC_ERR_TOO_LARGE -10    /* image needs more scratch than BC_NOALLOC_SCRATCH_BYTES */
+int bc_compress_bc7_device_noalloc(const bc_bc7_settings* settings, const uint8_t* rgba_dev,
+                                   size_t rgba_len, uint8_t* blocks_dev, size_t blocks_len,
+                                   uint32_t width, uint32_t height, size_t stride_bytes,
+                                   void* stream);
+
 /* ---- decode --------------------------------------------------------------
  * decode::decompress_blocks_as_rgba8 (src/decode.rs:336-387): blocks_len must
  * equal bc_blocks_byte_size(variant, w, h) and rgba_len must equal w*h*4.
