@@ -34,7 +34,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W = H = 2048
-METRIC = "BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
+# Algorithmic work per 4x4 block: FP32 operations of the reference encoder
+# (add/sub/mul/div/sqrt/abs/min/max/compare/convert), measured with the
+# op-counting build of the CPU restatement (`python -m oracle.count_ops`,
+# 2048 sampled blocks of this workload's content).
+OPS_PER_BLOCK = {"bc7_alpha_basic": 354530.4, "bc3": 1155.0, "bc4": 101.4, "bc5": 202.3}
+SMS, FP32_LANES_PER_SM = 148, 128
+# DRAM bytes (read + write) of one BC7 encode of this workload, summed over
+# the pipeline's launches, from an ncu capture (profiles/bc7_pipeline_2048.md).
+BC7_DRAM_BYTES_PER_LAUNCH = None
+METRIC ="BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
 WORKLOAD = "2048x2048 RGBA8 alpha texture: BC7 alpha_basic + BC3 + BC4(R); 2048x2048 normal map: BC5"
 
 
@@ -292,11 +301,18 @@ def gpu_bench(args, world, rank, local):
     bc3_ms = sum(per_job["bc3"]) / len(per_job["bc3"])
     if rank == 0:
         per_variant = {name: W * H / (sum(ms) / len(ms) / 1e3) / 1e6 for name, ms in per_job.items()}
+        # BC7 is compute bound: algorithmic FP32 ops per launch / duration,
+        # against the FP32 issue rate (148 SMs x 128 lanes x max SM clock; the
+        # encoder's order-preserving arithmetic admits no FMA).
+        nblk = (W // 4) * (H // 4)
+        fp32_peak = SMS * FP32_LANES_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        achieved = OPS_PER_BLOCK["bc7_alpha_basic"] * nblk / (bc7_ms / 1e3) / 1e12
         roof = {
-            "kernel": "bc7_encode_kernel", "bound": "issue", "unit": "Gblock/s",
-            "achieved": (W // 4) * (H // 4) / (bc7_ms / 1e3) / 1e9,
-            "peak": None, "frac": None, "traffic": None,
-            "note": "compute (FP32/INT issue) bound; see profiles/ for the issue-rate fraction",
+            "kernel": "BC7 encode pipeline (bc7_prep/search/refine/mode45/mode6/select)", "bound": "fp32",
+            "unit": "TFLOP/s", "achieved": achieved, "peak": fp32_peak, "frac": achieved / fp32_peak,
+            "peak_source": "148 SMs x 128 FP32 lanes x %s sm_max_mhz (%s)" % (peaks.get("sm_max_mhz"), src),
+            "traffic": BC7_DRAM_BYTES_PER_LAUNCH, "algorithmic_ops_per_block": OPS_PER_BLOCK["bc7_alpha_basic"],
+            "ms_per_launch": bc7_ms,
         }
         bc3_bytes = W * H * 4 + (W // 4) * (H // 4) * 16
         hbm = {"kernel": "bc15_encode_kernel<BC3>", "bound": "hbm", "unit": "GB/s",

@@ -182,3 +182,37 @@ def encode_block_bc6h(block, settings):
     keep, sp = _settings_ptr(settings)
     lib().oracle_encode_block_bc6h(_ptr(np.ascontiguousarray(block, np.float32)), sp, _ptr(out))
     return out
+
+
+_count_lib = None
+
+
+def count_lib():
+    """The op-counting build (liboracle_count.so): per-block FP32 op counts of
+    the reference encoders, the algorithmic work of the BC6H/BC7 rooflines."""
+    global _count_lib
+    if _count_lib is None:
+        path = os.path.join(_HERE, "liboracle_count.so")
+        srcs = [f for f in os.listdir(_HERE) if f.endswith((".cpp", ".h"))] + ["Makefile"]
+        newest = max(os.path.getmtime(os.path.join(_HERE, f)) for f in srcs)
+        if not os.path.exists(path) or os.path.getmtime(path) < newest:
+            subprocess.run(["make", "-s", "-C", _HERE, "liboracle_count.so"], check=True)
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        for name, args in (("oracle_count_bc7", [P, P]), ("oracle_count_bc6h", [P, P]),
+                           ("oracle_count_bc1", [P]), ("oracle_count_bc3_alpha", [P])):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = ctypes.c_uint64
+        _count_lib = L
+    return _count_lib
+
+
+def count_ops(kind, block, settings=None):
+    """FP32 ops of one block: kind in bc1, bc3_alpha, bc6h, bc7."""
+    L = count_lib()
+    b = np.ascontiguousarray(block, dtype=np.float32)
+    if kind in ("bc1", "bc3_alpha"):
+        return getattr(L, "oracle_count_" + kind)(_ptr(b))
+    keep, sp = _settings_ptr(settings)
+    return getattr(L, "oracle_count_" + kind)(_ptr(b), sp)

@@ -5,17 +5,17 @@
 namespace oracle {
 
 // bc1_to_5.rs:157-192
-static void compute_covar_dc(const float block[64], float covar[6], float dc[3]) {
+static void compute_covar_dc(const real block[64], real covar[6], real dc[3]) {
     for (int p = 0; p < 3; p++) {
-        float acc = 0.0f;
+        real acc = 0.0f;
         for (int k = 0; k < 16; k++) acc += block[k + p * 16];
         dc[p] = acc / 16.0f;
     }
-    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, c3 = 0.0f, c4 = 0.0f, c5 = 0.0f;
+    real c0 = 0.0f, c1 = 0.0f, c2 = 0.0f, c3 = 0.0f, c4 = 0.0f, c5 = 0.0f;
     for (int k = 0; k < 16; k++) {
-        float rgb0 = block[k] - dc[0];
-        float rgb1 = block[k + 16] - dc[1];
-        float rgb2 = block[k + 32] - dc[2];
+        real rgb0 = block[k] - dc[0];
+        real rgb1 = block[k + 16] - dc[1];
+        real rgb2 = block[k + 32] - dc[2];
         c0 += rgb0 * rgb0;
         c1 += rgb0 * rgb1;
         c2 += rgb0 * rgb2;
@@ -32,24 +32,24 @@ static void compute_covar_dc(const float block[64], float covar[6], float dc[3])
 }
 
 // bc1_to_5.rs:194-198
-static void ssymv(float r[3], const float covar[6], const float a[3]) {
+static void ssymv(real r[3], const real covar[6], const real a[3]) {
     r[0] = covar[0] * a[0] + covar[1] * a[1] + covar[2] * a[2];
     r[1] = covar[1] * a[0] + covar[3] * a[1] + covar[4] * a[2];
     r[2] = covar[2] * a[0] + covar[4] * a[1] + covar[5] * a[2];
 }
 
 // bc1_to_5.rs:200-223
-static void compute_axis3(float axis[3], const float covar[6], int power_iterations) {
-    float a[3] = {1.0f, 1.0f, 1.0f};
+static void compute_axis3(real axis[3], const real covar[6], int power_iterations) {
+    real a[3] = {1.0f, 1.0f, 1.0f};
     for (int i = 0; i < power_iterations; i++) {
         ssymv(axis, covar, a);
         a[0] = axis[0];
         a[1] = axis[1];
         a[2] = axis[2];
         if (i % 2 == 1) {
-            float norm_sq = 0.0f;
+            real norm_sq = 0.0f;
             for (int p = 0; p < 3; p++) norm_sq += axis[p] * axis[p];
-            float rnorm = 1.0f / std::sqrt(norm_sq);
+            real rnorm = 1.0f / sqrt_r(norm_sq);
             for (int p = 0; p < 3; p++) a[p] *= rnorm;
         }
     }
@@ -59,13 +59,13 @@ static void compute_axis3(float axis[3], const float covar[6], int power_iterati
 }
 
 // bc1_to_5.rs:225-256
-static void pick_endpoints(const float block[64], float c0[3], float c1[3], const float axis[3],
-                           const float dc[3]) {
-    float min_dot = 256.0f * 256.0f;
-    float max_dot = 0.0f;
+static void pick_endpoints(const real block[64], real c0[3], real c1[3], const real axis[3],
+                           const real dc[3]) {
+    real min_dot = 256.0f * 256.0f;
+    real max_dot = 0.0f;
     for (int y = 0; y < 4; y++) {
         for (int x = 0; x < 4; x++) {
-            float dot = 0.0f;
+            real dot = 0.0f;
             for (int p = 0; p < 3; p++) dot += (block[p * 16 + y * 4 + x] - dc[p]) * axis[p];
             min_dot = fmin_r(min_dot, dot);
             max_dot = fmax_r(max_dot, dot);
@@ -75,9 +75,9 @@ static void pick_endpoints(const float block[64], float c0[3], float c1[3], cons
         min_dot -= 0.5f;
         max_dot += 0.5f;
     }
-    float norm_sq = 0.0f;
+    real norm_sq = 0.0f;
     for (int p = 0; p < 3; p++) norm_sq += axis[p] * axis[p];
-    float rnorm_sq = 1.0f / norm_sq;
+    real rnorm_sq = 1.0f / norm_sq;
     for (int p = 0; p < 3; p++) {
         c0[p] = clampf_r(dc[p] + min_dot * rnorm_sq * axis[p], 0.0f, 255.0f);
         c1[p] = clampf_r(dc[p] + max_dot * rnorm_sq * axis[p], 0.0f, 255.0f);
@@ -85,17 +85,17 @@ static void pick_endpoints(const float block[64], float c0[3], float c1[3], cons
 }
 
 // bc1_to_5.rs:258-266
-static void dec_rgb565(float c[3], int32_t p) {
+static void dec_rgb565(real c[3], int32_t p) {
     int32_t b5 = p & 31;
     int32_t g6 = (p >> 5) & 63;
     int32_t r5 = (p >> 11) & 31;
-    c[0] = (float)((r5 << 3) + (r5 >> 2));
-    c[1] = (float)((g6 << 2) + (g6 >> 4));
-    c[2] = (float)((b5 << 3) + (b5 >> 2));
+    c[0] = (real)((r5 << 3) + (r5 >> 2));
+    c[1] = (real)((g6 << 2) + (g6 >> 4));
+    c[2] = (real)((b5 << 3) + (b5 >> 2));
 }
 
 // bc1_to_5.rs:268-278
-static int32_t enc_rgb565(const float c[3]) {
+static int32_t enc_rgb565(const real c[3]) {
     int32_t r = f2i(c[0]);
     int32_t g = f2i(c[1]);
     int32_t b = f2i(c[2]);
@@ -106,22 +106,22 @@ static int32_t enc_rgb565(const float c[3]) {
 }
 
 // bc1_to_5.rs:280-321
-static uint32_t fast_quant(const float block[64], int32_t p0, int32_t p1) {
-    float c0[3], c1[3];
+static uint32_t fast_quant(const real block[64], int32_t p0, int32_t p1) {
+    real c0[3], c1[3];
     dec_rgb565(c0, p0);
     dec_rgb565(c1, p1);
-    float dir[3];
+    real dir[3];
     for (int p = 0; p < 3; p++) dir[p] = c1[p] - c0[p];
-    float sq_norm = 0.0f;
+    real sq_norm = 0.0f;
     for (int p = 0; p < 3; p++) sq_norm += dir[p] * dir[p];
-    float rsq_norm = 1.0f / sq_norm;
+    real rsq_norm = 1.0f / sq_norm;
     for (int p = 0; p < 3; p++) dir[p] *= rsq_norm * 3.0f;
-    float bias = 0.5f;
+    real bias = 0.5f;
     for (int p = 0; p < 3; p++) bias -= c0[p] * dir[p];
     uint32_t bits = 0;
     uint32_t scaler = 1;
     for (int k = 0; k < 16; k++) {
-        float dot = 0.0f;
+        real dot = 0.0f;
         for (int p = 0; p < 3; p++) dot += block[k + p * 16] * dir[p];
         int32_t q = clampi_r(f2i(dot + bias), 0, 3);
         bits += (uint32_t)q * scaler;
@@ -131,35 +131,35 @@ static uint32_t fast_quant(const float block[64], int32_t p0, int32_t p1) {
 }
 
 // bc1_to_5.rs:323-374
-static void bc1_refine(const float block[64], int32_t pe[2], uint32_t bits, const float dc[3]) {
-    float c0[3], c1[3];
+static void bc1_refine(const real block[64], int32_t pe[2], uint32_t bits, const real dc[3]) {
+    real c0[3], c1[3];
     if ((bits ^ (bits * 4u)) < 4) {
         for (int p = 0; p < 3; p++) {
             c0[p] = dc[p];
             c1[p] = dc[p];
         }
     } else {
-        float atb1[3] = {0.0f, 0.0f, 0.0f};
-        float sum_q = 0.0f;
-        float sum_qq = 0.0f;
+        real atb1[3] = {0.0f, 0.0f, 0.0f};
+        real sum_q = 0.0f;
+        real sum_qq = 0.0f;
         uint32_t shifted = bits;
         for (int k = 0; k < 16; k++) {
-            float q = (float)(shifted & 3);
+            real q = (real)(shifted & 3);
             shifted >>= 2;
-            float x = 3.0f - q;
+            real x = 3.0f - q;
             sum_q += q;
             sum_qq += q * q;
             for (int p = 0; p < 3; p++) atb1[p] += x * block[k + p * 16];
         }
-        float sum[3], atb2[3];
+        real sum[3], atb2[3];
         for (int p = 0; p < 3; p++) {
             sum[p] = dc[p] * 16.0f;
             atb2[p] = 3.0f * sum[p] - atb1[p];
         }
-        float cxx = 16.0f * 9.0f - 2.0f * 3.0f * sum_q + sum_qq;
-        float cyy = sum_qq;
-        float cxy = 3.0f * sum_q - sum_qq;
-        float scale = 3.0f * (1.0f / (cxx * cyy - cxy * cxy));
+        real cxx = 16.0f * 9.0f - 2.0f * 3.0f * sum_q + sum_qq;
+        real cyy = sum_qq;
+        real cxy = 3.0f * sum_q - sum_qq;
+        real scale = 3.0f * (1.0f / (cxx * cyy - cxy * cxy));
         for (int p = 0; p < 3; p++) {
             c0[p] = (atb1[p] * cyy - atb2[p] * cxy) * scale;
             c1[p] = (atb2[p] * cxx - atb1[p] * cxy) * scale;
@@ -181,18 +181,18 @@ static uint32_t fix_qbits(uint32_t qbits) {
 }
 
 // bc1_to_5.rs:386-429
-void bc1_core(const float block[64], uint32_t data[2]) {
+void bc1_core(const real block[64], uint32_t data[2]) {
     const int power_iterations = 4;
     const int refine_iterations = 1;
-    float covar[6], dc[3];
+    real covar[6], dc[3];
     compute_covar_dc(block, covar, dc);
-    const float eps = 1.1920929e-7f;  // f32::EPSILON
+    const real eps = 1.1920929e-7f;  // f32::EPSILON
     covar[0] += eps;
     covar[3] += eps;
     covar[5] += eps;
-    float axis[3];
+    real axis[3];
     compute_axis3(axis, covar, power_iterations);
-    float c0[3], c1[3];
+    real c0[3], c1[3];
     pick_endpoints(block, c0, c1, axis, dc);
     int32_t p[2];
     p[0] = enc_rgb565(c0);
@@ -218,18 +218,18 @@ void bc1_core(const float block[64], uint32_t data[2]) {
 }
 
 // bc1_to_5.rs:431-472
-void bc3_alpha(const float block[64], uint32_t data[2]) {
-    float ep[2] = {255.0f, 0.0f};
+void bc3_alpha(const real block[64], uint32_t data[2]) {
+    real ep[2] = {255.0f, 0.0f};
     for (int k = 0; k < 16; k++) {
         ep[0] = fmin_r(ep[0], block[48 + k]);
         ep[1] = fmax_r(ep[1], block[48 + k]);
     }
     if (ep[0] == ep[1]) ep[1] = ep[0] + 0.1f;
     uint32_t qblock[2] = {0, 0};
-    float scale = 7.0f / (ep[1] - ep[0]);
+    real scale = 7.0f / (ep[1] - ep[0]);
     for (int k = 0; k < 16; k++) {
-        float v = block[48 + k];
-        float proj = (v - ep[0]) * scale + 0.5f;
+        real v = block[48 + k];
+        real proj = (v - ep[0]) * scale + 0.5f;
         int32_t q = clampi_r(f2i(proj), 0, 7);
         q = 7 - q;
         if (q > 0) q += 1;

@@ -7,11 +7,11 @@ namespace oracle {
 namespace {
 
 struct BC6H {  // bc6h.rs:4-17
-    float block[64];
+    real block[64];
     uint32_t data[5];
-    float best_err;
-    float rgb_bounds[6];
-    float max_span;
+    real best_err;
+    real rgb_bounds[6];
+    real max_span;
     uint32_t max_span_idx;
     uint32_t mode;
     uint32_t epb;
@@ -25,8 +25,8 @@ uint32_t get_mode_prefix(uint32_t mode) {
     return t[mode];
 }
 
-float get_span(uint32_t mode) {
-    static const float t[14] = {
+real get_span(uint32_t mode) {
+    static const real t[14] = {
         0.9f * 65535.0f / 64.0f, 0.9f * 65535.0f / 4.0f, 0.8f * 65535.0f / 256.0f, -1.0f, -1.0f,
         0.9f * 65535.0f / 32.0f, 0.9f * 65535.0f / 16.0f, -1.0f, -1.0f, 65535.0f, 65535.0f,
         0.95f * 65535.0f / 8.0f, 0.95f * 65535.0f / 32.0f, 6.0f,
@@ -40,32 +40,32 @@ uint32_t get_mode_bits(uint32_t mode) {
 }
 
 // bc6h.rs:166-173
-void ep_quant_bc6h_8(BC6H& s, const float ep[8], uint32_t bits, uint32_t pairs) {
+void ep_quant_bc6h_8(BC6H& s, const real ep[8], uint32_t bits, uint32_t pairs) {
     int32_t levels = 1 << bits;
     for (uint32_t i = 0; i < 8 * pairs; i++) {
-        int32_t v = f2i(ep[i] / (256.0f * 256.0f - 1.0f) * (float)(levels - 1) + 0.5f);
+        int32_t v = f2i(ep[i] / (256.0f * 256.0f - 1.0f) * (real)(levels - 1) + 0.5f);
         s.qbounds[i] = clampi_r(v, 0, levels - 1);
     }
 }
 
 // bc6h.rs:175-197
-void compute_qbounds_core(BC6H& s, const float rgb_span[3]) {
-    float bounds[8] = {0};
+void compute_qbounds_core(BC6H& s, const real rgb_span[3]) {
+    real bounds[8] = {0};
     for (int p = 0; p < 3; p++) {
-        float middle = (s.rgb_bounds[p] + s.rgb_bounds[3 + p]) / 2.0f;
+        real middle = (s.rgb_bounds[p] + s.rgb_bounds[3 + p]) / 2.0f;
         bounds[p] = middle - rgb_span[p] / 2.0f;
         bounds[4 + p] = middle + rgb_span[p] / 2.0f;
     }
     ep_quant_bc6h_8(s, bounds, s.epb, 1);
 }
 
-void compute_qbounds(BC6H& s, float span) {
-    float r[3] = {span, span, span};
+void compute_qbounds(BC6H& s, real span) {
+    real r[3] = {span, span, span};
     compute_qbounds_core(s, r);
 }
 
-void compute_qbounds2(BC6H& s, float span, uint32_t max_span_idx) {
-    float r[3] = {span, span, span};
+void compute_qbounds2(BC6H& s, real span, uint32_t max_span_idx) {
+    real r[3] = {span, span, span};
     if (max_span_idx < 3) r[max_span_idx] *= 2.0f;
     compute_qbounds_core(s, r);
 }
@@ -79,16 +79,16 @@ uint32_t unpack_to_uf16(uint32_t v, uint32_t bits) {
 }
 
 // bc6h.rs:213-239
-void ep_quant_dequant_bc6h(const BC6H& s, int32_t qep[24], float ep[24], uint32_t pairs) {
+void ep_quant_dequant_bc6h(const BC6H& s, int32_t qep[24], real ep[24], uint32_t pairs) {
     uint32_t bits = s.epb;
     int32_t levels = 1 << bits;
     for (uint32_t i = 0; i < 8 * pairs; i++) {
-        int32_t v = f2i(ep[i] / (256.0f * 256.0f - 1.0f) * (float)(levels - 1) + 0.5f);
+        int32_t v = f2i(ep[i] / (256.0f * 256.0f - 1.0f) * (real)(levels - 1) + 0.5f);
         qep[i] = clampi_r(v, 0, levels - 1);
     }
     for (uint32_t i = 0; i < 2 * pairs; i++)
         for (int p = 0; p < 3; p++) qep[i * 4 + p] = clampi_r(qep[i * 4 + p], s.qbounds[p], s.qbounds[4 + p]);
-    for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (float)unpack_to_uf16((uint32_t)qep[i], bits);
+    for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (real)unpack_to_uf16((uint32_t)qep[i], bits);
 }
 
 inline uint32_t bit_at(int32_t v, uint32_t pos) { return (uint32_t)((v >> pos) & 1); }
@@ -400,9 +400,9 @@ void bc6h_code_1p(BC6H& s, int32_t qep[24], uint32_t qblock[2], uint32_t mode) {
 }
 
 // bc6h.rs:304-324
-float bc6h_enc_2p_part_fast(const BC6H& s, int32_t qep[24], uint32_t qblock[2], int32_t part_id) {
+real bc6h_enc_2p_part_fast(const BC6H& s, int32_t qep[24], uint32_t qblock[2], int32_t part_id) {
     uint32_t pattern = get_pattern(part_id);
-    float ep[24] = {0};
+    real ep[24] = {0};
     for (uint32_t j = 0; j < 2; j++) {
         uint32_t mask = get_pattern_mask(part_id, j);
         block_segment_core(ep + j * 8, s.block, mask, 3);
@@ -418,12 +418,12 @@ void bc6h_enc_2p_list(BC6H& s, const int32_t part_list[32], uint32_t part_count)
     int32_t best_qep[24] = {0};
     uint32_t best_qblock[2] = {0, 0};
     int32_t best_part_id = -1;
-    float best_err = INFINITY;
+    real best_err = INFINITY;
     for (uint32_t part = 0; part < part_count; part++) {
         int32_t part_id = part_list[part] & 31;
         int32_t qep[24] = {0};
         uint32_t qblock[2] = {0, 0};
-        float err = bc6h_enc_2p_part_fast(s, qep, qblock, part_id);
+        real err = bc6h_enc_2p_part_fast(s, qep, qblock, part_id);
         if (err < best_err) {
             std::memcpy(best_qep, qep, sizeof(int32_t) * 16);
             best_qblock[0] = qblock[0];
@@ -436,7 +436,7 @@ void bc6h_enc_2p_list(BC6H& s, const int32_t part_list[32], uint32_t part_count)
     // Rust code would panic on the -1 index.
     if (best_part_id < 0) return;
     for (uint32_t it = 0; it < s.settings->refine_iterations_2p; it++) {
-        float ep[24] = {0};
+        real ep[24] = {0};
         for (uint32_t j = 0; j < 2; j++) {
             uint32_t mask = get_pattern_mask(best_part_id, j);
             opt_endpoints(ep + j * 8, s.block, bits, best_qblock, mask, channels);
@@ -445,7 +445,7 @@ void bc6h_enc_2p_list(BC6H& s, const int32_t part_list[32], uint32_t part_count)
         uint32_t qblock[2] = {0, 0};
         ep_quant_dequant_bc6h(s, qep, ep, 2);
         uint32_t pattern = get_pattern(best_part_id);
-        float err = block_quant(qblock, s.block, bits, ep, pattern, channels);
+        real err = block_quant(qblock, s.block, bits, ep, pattern, channels);
         if (err < best_err) {
             std::memcpy(best_qep, qep, sizeof(int32_t) * 16);
             best_qblock[0] = qblock[0];
@@ -461,12 +461,12 @@ void bc6h_enc_2p_list(BC6H& s, const int32_t part_list[32], uint32_t part_count)
 
 // bc6h.rs:288-302
 void bc6h_enc_2p(BC6H& s) {
-    float full_stats[15] = {0};
+    real full_stats[15] = {0};
     compute_stats_masked(full_stats, s.block, 0xFFFFFFFFu, 3);
     int32_t part_list[32];
     for (int32_t part = 0; part < 32; part++) {
         uint32_t mask = get_pattern_mask(part, 0);
-        float bound12 = block_pca_bound_split(s.block, mask, full_stats, 3);
+        real bound12 = block_pca_bound_split(s.block, mask, full_stats, 3);
         int32_t bound = f2i(bound12);
         part_list[part] = part + bound * 64;
     }
@@ -476,12 +476,12 @@ void bc6h_enc_2p(BC6H& s) {
 
 // bc6h.rs:390-412
 void bc6h_enc_1p(BC6H& s) {
-    float ep[24] = {0};
+    real ep[24] = {0};
     block_segment_core(ep, s.block, 0xFFFFFFFFu, 3);
     int32_t qep[24] = {0};
     ep_quant_dequant_bc6h(s, qep, ep, 1);
     uint32_t qblock[2] = {0, 0};
-    float err = block_quant(qblock, s.block, 4, ep, 0, 3);
+    real err = block_quant(qblock, s.block, 4, ep, 0, 3);
     for (uint32_t it = 0; it < s.settings->refine_iterations_1p; it++) {
         opt_endpoints(ep, s.block, 4, qblock, 0xFFFFFFFFu, 3);
         ep_quant_dequant_bc6h(s, qep, ep, 1);
@@ -494,10 +494,10 @@ void bc6h_enc_1p(BC6H& s) {
 }
 
 // bc6h.rs:414-446
-void bc6h_test_mode(BC6H& s, uint32_t mode, bool enc, float margin) {
+void bc6h_test_mode(BC6H& s, uint32_t mode, bool enc, real margin) {
     uint32_t mode_bits = get_mode_bits(mode);
-    float span = get_span(mode);
-    float max_span = s.max_span;
+    real span = get_span(mode);
+    real max_span = s.max_span;
     uint32_t max_span_idx = s.max_span_idx;
     if (max_span * margin > span) return;
     if (mode >= 10) {
@@ -521,12 +521,12 @@ void bc6h_test_mode(BC6H& s, uint32_t mode, bool enc, float margin) {
 // bc6h.rs:793-819
 void bc6h_setup(BC6H& s) {
     for (int p = 0; p < 3; p++) {
-        s.rgb_bounds[p] = (float)0xFFFF;
+        s.rgb_bounds[p] = (real)0xFFFF;
         s.rgb_bounds[3 + p] = 0.0f;
     }
     for (int p = 0; p < 3; p++) {
         for (int k = 0; k < 16; k++) {
-            float value = (s.block[p * 16 + k] / 31.0f) * 64.0f;
+            real value = (s.block[p * 16 + k] / 31.0f) * 64.0f;
             s.block[p * 16 + k] = value;
             s.rgb_bounds[p] = fmin_r(s.rgb_bounds[p], value);
             s.rgb_bounds[3 + p] = fmax_r(s.rgb_bounds[3 + p], value);
@@ -535,7 +535,7 @@ void bc6h_setup(BC6H& s) {
     s.max_span = 0.0f;
     s.max_span_idx = 0;
     for (uint32_t p = 0; p < 3; p++) {
-        float span = s.rgb_bounds[3 + p] - s.rgb_bounds[p];
+        real span = s.rgb_bounds[3 + p] - s.rgb_bounds[p];
         if (span > s.max_span) {
             s.max_span_idx = p;
             s.max_span = span;
@@ -547,7 +547,7 @@ void bc6h_setup(BC6H& s) {
 
 // bc6h.rs:821-860 (compress_bc6h_core), fed by the planar block that
 // load_block_interleaved_16bit (bc6h.rs:73-97) builds: f16 bit patterns as f32.
-void bc6h_encode_block(const float block_in[64], const BC6HSettings* settings, uint32_t out[4]) {
+void bc6h_encode_block(const real block_in[64], const BC6HSettings* settings, uint32_t out[4]) {
     BC6H s;
     std::memcpy(s.block, block_in, sizeof(s.block));
     std::memset(s.data, 0, sizeof(s.data));

@@ -16,10 +16,10 @@ struct Mode45Parameters {  // bc7.rs:4-12
 };
 
 struct BC7 {  // bc7.rs:14-36
-    float block[64];
+    real block[64];
     uint32_t data[5];
-    float best_err;
-    float opaque_err;
+    real best_err;
+    real opaque_err;
     const BC7Settings* settings;
 };
 
@@ -32,7 +32,7 @@ int32_t unpack_to_byte(int32_t v, uint32_t bits) {
 }
 
 // bc7.rs:102-148
-void ep_quant0367(int32_t* qep, const float* ep, uint32_t mode, uint32_t channels) {
+void ep_quant0367(int32_t* qep, const real* ep, uint32_t mode, uint32_t channels) {
     int32_t bits = mode == 0 ? 4 : (mode == 7 ? 5 : 7);
     int32_t levels = 1 << bits;
     int32_t levels2 = levels * 2 - 1;
@@ -40,15 +40,15 @@ void ep_quant0367(int32_t* qep, const float* ep, uint32_t mode, uint32_t channel
         int32_t qep_b[8];
         for (int b = 0; b < 2; b++) {
             for (int p = 0; p < 4; p++) {
-                int32_t v = f2i(((ep[i * 4 + p] / 255.0f * (float)levels2 - (float)b) / 2.0f + 0.5f)) * 2 + b;
+                int32_t v = f2i(((ep[i * 4 + p] / 255.0f * (real)levels2 - (real)b) / 2.0f + 0.5f)) * 2 + b;
                 qep_b[b * 4 + p] = clampi_r(v, b, levels2 - 1 + b);
             }
         }
-        float ep_b[8];
-        for (int j = 0; j < 8; j++) ep_b[j] = (float)qep_b[j];
+        real ep_b[8];
+        for (int j = 0; j < 8; j++) ep_b[j] = (real)qep_b[j];
         if (mode == 0)
-            for (int j = 0; j < 8; j++) ep_b[j] = (float)unpack_to_byte(qep_b[j], 5);
-        float err0 = 0.0f, err1 = 0.0f;
+            for (int j = 0; j < 8; j++) ep_b[j] = (real)unpack_to_byte(qep_b[j], 5);
+        real err0 = 0.0f, err1 = 0.0f;
         for (uint32_t p = 0; p < channels; p++) {
             err0 += sq(ep[i * 4 + p] - ep_b[p]);
             err1 += sq(ep[i * 4 + p] - ep_b[4 + p]);
@@ -58,17 +58,17 @@ void ep_quant0367(int32_t* qep, const float* ep, uint32_t mode, uint32_t channel
 }
 
 // bc7.rs:150-178
-void ep_quant1(int32_t* qep, const float* ep) {
+void ep_quant1(int32_t* qep, const real* ep) {
     int32_t qep_b[16];
     for (int b = 0; b < 2; b++) {
         for (int i = 0; i < 8; i++) {
-            int32_t v = f2i(((ep[i] / 255.0f * 127.0f - (float)b) / 2.0f + 0.5f)) * 2 + b;
+            int32_t v = f2i(((ep[i] / 255.0f * 127.0f - (real)b) / 2.0f + 0.5f)) * 2 + b;
             qep_b[b * 8 + i] = clampi_r(v, b, 126 + b);
         }
     }
-    float ep_b[16];
-    for (int k = 0; k < 16; k++) ep_b[k] = (float)unpack_to_byte(qep_b[k], 7);
-    float err0 = 0.0f, err1 = 0.0f;
+    real ep_b[16];
+    for (int k = 0; k < 16; k++) ep_b[k] = (real)unpack_to_byte(qep_b[k], 7);
+    real err0 = 0.0f, err1 = 0.0f;
     for (int j = 0; j < 2; j++) {
         for (int p = 0; p < 3; p++) {
             err0 += sq(ep[j * 4 + p] - ep_b[j * 4 + p]);
@@ -79,17 +79,17 @@ void ep_quant1(int32_t* qep, const float* ep) {
 }
 
 // bc7.rs:180-189
-void ep_quant245(int32_t* qep, const float* ep, uint32_t mode) {
+void ep_quant245(int32_t* qep, const real* ep, uint32_t mode) {
     int32_t bits = mode == 5 ? 7 : 5;
     int32_t levels = 1 << bits;
     for (int i = 0; i < 8; i++) {
-        int32_t v = f2i(ep[i] / 255.0f * (float)(levels - 1) + 0.5f);
+        int32_t v = f2i(ep[i] / 255.0f * (real)(levels - 1) + 0.5f);
         qep[i] = clampi_r(v, 0, levels - 1);
     }
 }
 
 // bc7.rs:191-208
-void ep_quant(int32_t* qep, const float* ep, uint32_t mode, uint32_t channels) {
+void ep_quant(int32_t* qep, const real* ep, uint32_t mode, uint32_t channels) {
     uint32_t pairs = kPairsTable[mode];
     if (mode == 0 || mode == 3 || mode == 6 || mode == 7) {
         for (uint32_t i = 0; i < pairs; i++) ep_quant0367(qep + i * 8, ep + i * 8, mode, channels);
@@ -101,53 +101,53 @@ void ep_quant(int32_t* qep, const float* ep, uint32_t mode, uint32_t channels) {
 }
 
 // bc7.rs:210-232
-void ep_dequant(float* ep, const int32_t* qep, uint32_t mode) {
+void ep_dequant(real* ep, const int32_t* qep, uint32_t mode) {
     uint32_t pairs = kPairsTable[mode];
     if (mode == 3 || mode == 6) {
-        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (float)qep[i];
+        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (real)qep[i];
     } else if (mode == 1 || mode == 5) {
-        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (float)unpack_to_byte(qep[i], 7);
+        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (real)unpack_to_byte(qep[i], 7);
     } else if (mode == 0 || mode == 2 || mode == 4) {
-        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (float)unpack_to_byte(qep[i], 5);
+        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (real)unpack_to_byte(qep[i], 5);
     } else if (mode == 7) {
-        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (float)unpack_to_byte(qep[i], 6);
+        for (uint32_t i = 0; i < 8 * pairs; i++) ep[i] = (real)unpack_to_byte(qep[i], 6);
     }
 }
 
 // bc7.rs:234-237
-void ep_quant_dequant(int32_t* qep, float* ep, uint32_t mode, uint32_t channels) {
+void ep_quant_dequant(int32_t* qep, real* ep, uint32_t mode, uint32_t channels) {
     ep_quant(qep, ep, mode, channels);
     ep_dequant(ep, qep, mode);
 }
 
 // bc7.rs:268-276
-void channel_quant_dequant(int32_t qep[2], float ep[2], uint32_t epbits) {
+void channel_quant_dequant(int32_t qep[2], real ep[2], uint32_t epbits) {
     int32_t elevels = 1 << epbits;
     for (int i = 0; i < 2; i++) {
-        int32_t v = f2i(ep[i] / 255.0f * (float)(elevels - 1) + 0.5f);
+        int32_t v = f2i(ep[i] / 255.0f * (real)(elevels - 1) + 0.5f);
         qep[i] = clampi_r(v, 0, elevels - 1);
-        ep[i] = (float)unpack_to_byte(qep[i], epbits);
+        ep[i] = (real)unpack_to_byte(qep[i], epbits);
     }
 }
 
 // bc7.rs:278-320
-float channel_opt_quant(uint32_t qblock[2], const float cb[16], uint32_t bits, const float ep[2]) {
+real channel_opt_quant(uint32_t qblock[2], const real cb[16], uint32_t bits, const real ep[2]) {
     int32_t levels = 1 << bits;
     qblock[0] = 0;
     qblock[1] = 0;
-    float total_err = 0.0f;
+    real total_err = 0.0f;
     for (int k = 0; k < 16; k++) {
-        float proj = (cb[k] - ep[0]) / (ep[1] - ep[0] + 0.001f);
-        int32_t q1 = f2i(proj * (float)levels + 0.5f);
+        real proj = (cb[k] - ep[0]) / (ep[1] - ep[0] + 0.001f);
+        int32_t q1 = f2i(proj * (real)levels + 0.5f);
         int32_t q1c = clampi_r(q1, 1, levels - 1);
-        float err0 = 0.0f, err1 = 0.0f;
+        real err0 = 0.0f, err1 = 0.0f;
         int32_t w0 = get_unquant_value(bits, q1c - 1);
         int32_t w1 = get_unquant_value(bits, q1c);
-        float dec_v0 = (float)(((64 - w0) * f2i(ep[0]) + w0 * f2i(ep[1]) + 32) / 64);
-        float dec_v1 = (float)(((64 - w1) * f2i(ep[0]) + w1 * f2i(ep[1]) + 32) / 64);
+        real dec_v0 = (real)(((64 - w0) * f2i(ep[0]) + w0 * f2i(ep[1]) + 32) / 64);
+        real dec_v1 = (real)(((64 - w1) * f2i(ep[0]) + w1 * f2i(ep[1]) + 32) / 64);
         err0 += sq(dec_v0 - cb[k]);
         err1 += sq(dec_v1 - cb[k]);
-        float best_err = err0 < err1 ? err0 : err1;
+        real best_err = err0 < err1 ? err0 : err1;
         int32_t best_q = err0 < err1 ? q1c - 1 : q1c;
         qblock[k / 8] |= ((uint32_t)best_q) << (4 * (k % 8));
         total_err += best_err;
@@ -156,48 +156,48 @@ float channel_opt_quant(uint32_t qblock[2], const float cb[16], uint32_t bits, c
 }
 
 // bc7.rs:322-369
-void channel_opt_endpoints(float ep[2], const float cb[16], uint32_t bits, const uint32_t qblock[2]) {
+void channel_opt_endpoints(real ep[2], const real cb[16], uint32_t bits, const uint32_t qblock[2]) {
     int32_t levels = 1 << bits;
-    float atb1 = 0.0f, sum_q = 0.0f, sum_qq = 0.0f, sum = 0.0f;
+    real atb1 = 0.0f, sum_q = 0.0f, sum_qq = 0.0f, sum = 0.0f;
     for (int k1 = 0; k1 < 2; k1++) {
         uint32_t qbits_shifted = qblock[k1];
         for (int k2 = 0; k2 < 8; k2++) {
             int k = k1 * 8 + k2;
-            float q = (float)(qbits_shifted & 15);
+            real q = (real)(qbits_shifted & 15);
             qbits_shifted >>= 4;
-            float x = (float)(levels - 1) - q;
+            real x = (real)(levels - 1) - q;
             sum_q += q;
             sum_qq += q * q;
             sum += cb[k];
             atb1 += x * cb[k];
         }
     }
-    float lm1 = (float)(levels - 1);
-    float atb2 = lm1 * sum - atb1;
-    float cxx = 16.0f * sq(lm1) - 2.0f * lm1 * sum_q + sum_qq;
-    float cyy = sum_qq;
-    float cxy = lm1 * sum_q - sum_qq;
-    float scale = lm1 / (cxx * cyy - cxy * cxy);
+    real lm1 = (real)(levels - 1);
+    real atb2 = lm1 * sum - atb1;
+    real cxx = 16.0f * sq(lm1) - 2.0f * lm1 * sum_q + sum_qq;
+    real cyy = sum_qq;
+    real cxy = lm1 * sum_q - sum_qq;
+    real scale = lm1 / (cxx * cyy - cxy * cxy);
     ep[0] = (atb1 * cyy - atb2 * cxy) * scale;
     ep[1] = (atb2 * cxx - atb1 * cxy) * scale;
     ep[0] = clampf_r(ep[0], 0.0f, 255.0f);
     ep[1] = clampf_r(ep[1], 0.0f, 255.0f);
-    if (std::fabs(cxx * cyy - cxy * cxy) < 0.001f) {
+    if (fabs_r(cxx * cyy - cxy * cxy) < 0.001f) {
         ep[0] = sum / 16.0f;
         ep[1] = ep[0];
     }
 }
 
 // bc7.rs:239-266
-float opt_channel(const BC7& s, uint32_t qblock[2], int32_t qep[2], const float cb[16], uint32_t bits,
+real opt_channel(const BC7& s, uint32_t qblock[2], int32_t qep[2], const real cb[16], uint32_t bits,
                   uint32_t epbits) {
-    float ep[2] = {255.0f, 0.0f};
+    real ep[2] = {255.0f, 0.0f};
     for (int k = 0; k < 16; k++) {
         ep[0] = fmin_r(ep[0], cb[k]);
         ep[1] = fmax_r(ep[1], cb[k]);
     }
     channel_quant_dequant(qep, ep, epbits);
-    float err = channel_opt_quant(qblock, cb, bits, ep);
+    real err = channel_opt_quant(qblock, cb, bits, ep);
     for (uint32_t it = 0; it < s.settings->refine_iterations_channel; it++) {
         channel_opt_endpoints(ep, cb, bits, qblock);
         channel_quant_dequant(qep, ep, epbits);
@@ -207,7 +207,7 @@ float opt_channel(const BC7& s, uint32_t qblock[2], int32_t qep[2], const float 
 }
 
 // bc7.rs:371-379
-void block_segment(float* ep, const float block[64], uint32_t mask, uint32_t channels) {
+void block_segment(real* ep, const real block[64], uint32_t mask, uint32_t channels) {
     block_segment_core(ep, block, mask, channels);
     for (int i = 0; i < 2; i++)
         for (uint32_t p = 0; p < channels; p++) ep[4 * i + p] = clampf_r(ep[4 * i + p], 0.0f, 255.0f);
@@ -299,13 +299,13 @@ void bc7_code_mode6(BC7& s, int32_t* qep, uint32_t qblock[2]) {
 }
 
 // bc7.rs:517-538
-float bc7_enc_mode01237_part_fast(const BC7& s, int32_t qep[24], uint32_t qblock[2], int32_t part_id,
+real bc7_enc_mode01237_part_fast(const BC7& s, int32_t qep[24], uint32_t qblock[2], int32_t part_id,
                                   uint32_t mode) {
     uint32_t pattern = get_pattern(part_id);
     uint32_t bits = (mode == 0 || mode == 1) ? 3 : 2;
     uint32_t pairs = (mode == 0 || mode == 2) ? 3 : 2;
     uint32_t channels = mode == 7 ? 4 : 3;
-    float ep[24] = {0};
+    real ep[24] = {0};
     for (uint32_t j = 0; j < pairs; j++) {
         uint32_t mask = get_pattern_mask(part_id, j);
         block_segment(ep + j * 8, s.block, mask, channels);
@@ -323,13 +323,13 @@ void bc7_enc_mode01237(BC7& s, uint32_t mode, const int32_t part_list[64], uint3
     int32_t best_qep[24] = {0};
     uint32_t best_qblock[2] = {0, 0};
     int32_t best_part_id = -1;
-    float best_err = INFINITY;
+    real best_err = INFINITY;
     for (uint32_t i = 0; i < part_count; i++) {
         int32_t part_id = part_list[i] & 63;
         part_id = pairs == 3 ? part_id + 64 : part_id;
         int32_t qep[24] = {0};
         uint32_t qblock[2] = {0, 0};
-        float err = bc7_enc_mode01237_part_fast(s, qep, qblock, part_id, mode);
+        real err = bc7_enc_mode01237_part_fast(s, qep, qblock, part_id, mode);
         if (err < best_err) {
             std::memcpy(best_qep, qep, sizeof(int32_t) * 8 * pairs);
             best_qblock[0] = qblock[0];
@@ -343,7 +343,7 @@ void bc7_enc_mode01237(BC7& s, uint32_t mode, const int32_t part_list[64], uint3
     if (best_part_id < 0) return;
     uint32_t refine_iterations = s.settings->refine_iterations[mode];
     for (uint32_t it = 0; it < refine_iterations; it++) {
-        float ep[24] = {0};
+        real ep[24] = {0};
         for (uint32_t j = 0; j < pairs; j++) {
             uint32_t mask = get_pattern_mask(best_part_id, j);
             opt_endpoints(ep + j * 8, s.block, bits, best_qblock, mask, channels);
@@ -352,7 +352,7 @@ void bc7_enc_mode01237(BC7& s, uint32_t mode, const int32_t part_list[64], uint3
         uint32_t qblock[2] = {0, 0};
         ep_quant_dequant(qep, ep, mode, channels);
         uint32_t pattern = get_pattern(best_part_id);
-        float err = block_quant(qblock, s.block, bits, ep, pattern, channels);
+        real err = block_quant(qblock, s.block, bits, ep, pattern, channels);
         if (err < best_err) {
             std::memcpy(best_qep, qep, sizeof(int32_t) * 8 * pairs);
             best_qblock[0] = qblock[0];
@@ -378,12 +378,12 @@ void bc7_enc_mode02(BC7& s) {
 // bc7.rs:622-655
 void bc7_enc_mode13(BC7& s) {
     if (s.settings->fast_skip_threshold_mode1 == 0 && s.settings->fast_skip_threshold_mode3 == 0) return;
-    float full_stats[15] = {0};
+    real full_stats[15] = {0};
     compute_stats_masked(full_stats, s.block, 0xFFFFFFFFu, 3);
     int32_t part_list[64];
     for (int32_t part = 0; part < 64; part++) {
         uint32_t mask = get_pattern_mask(part, 0);
-        float bound12 = block_pca_bound_split(s.block, mask, full_stats, 3);
+        real bound12 = block_pca_bound_split(s.block, mask, full_stats, 3);
         int32_t bound = f2i(bound12);
         part_list[part] = part + bound * 64;
     }
@@ -396,7 +396,7 @@ void bc7_enc_mode13(BC7& s) {
 }
 
 // bc7.rs:657-733
-void bc7_enc_mode45_candidate(const BC7& s, Mode45Parameters& best_candidate, float* best_err, uint32_t mode,
+void bc7_enc_mode45_candidate(const BC7& s, Mode45Parameters& best_candidate, real* best_err, uint32_t mode,
                               uint32_t rotation, uint32_t swap) {
     uint32_t bits = 2;
     uint32_t abits = 2;
@@ -409,7 +409,7 @@ void bc7_enc_mode45_candidate(const BC7& s, Mode45Parameters& best_candidate, fl
         bits = 3;
         abits = 2;
     }
-    float candidate_block[64] = {0};
+    real candidate_block[64] = {0};
     for (int k = 0; k < 16; k++) {
         for (int p = 0; p < 3; p++) candidate_block[k + p * 16] = s.block[k + p * 16];
         if (rotation < 3) {
@@ -417,19 +417,19 @@ void bc7_enc_mode45_candidate(const BC7& s, Mode45Parameters& best_candidate, fl
             if (s.settings->channels == 3) candidate_block[k + rotation * 16] = 255.0f;
         }
     }
-    float ep[8] = {0};
+    real ep[8] = {0};
     block_segment(ep, candidate_block, 0xFFFFFFFFu, 3);
     int32_t qep[8] = {0};
     ep_quant_dequant(qep, ep, mode, 3);
     uint32_t qblock[2] = {0, 0};
-    float err = block_quant(qblock, candidate_block, bits, ep, 0, 3);
+    real err = block_quant(qblock, candidate_block, bits, ep, 0, 3);
     uint32_t refine_iterations = s.settings->refine_iterations[mode];
     for (uint32_t it = 0; it < refine_iterations; it++) {
         opt_endpoints(ep, candidate_block, bits, qblock, 0xFFFFFFFFu, 3);
         ep_quant_dequant(qep, ep, mode, 3);
         err = block_quant(qblock, candidate_block, bits, ep, 0, 3);
     }
-    float channel_data[16];
+    real channel_data[16];
     for (int k = 0; k < 16; k++) channel_data[k] = s.block[k + rotation * 16];
     int32_t aqep[2] = {0, 0};
     uint32_t aqblock[2] = {0, 0};
@@ -451,7 +451,7 @@ void bc7_enc_mode45_candidate(const BC7& s, Mode45Parameters& best_candidate, fl
 // bc7.rs:735-760
 void bc7_enc_mode45(BC7& s) {
     Mode45Parameters best_candidate;
-    float best_err = s.best_err;
+    real best_err = s.best_err;
     uint32_t channel0 = s.settings->mode45_channel0;
     for (uint32_t p = channel0; p < s.settings->channels; p++) {
         bc7_enc_mode45_candidate(s, best_candidate, &best_err, 4, p, 0);
@@ -474,7 +474,7 @@ void bc7_enc_mode6(BC7& s) {
     const uint32_t mode = 6;
     const uint32_t bits = 4;
     uint32_t channels = s.settings->channels;
-    float ep[8] = {0};
+    real ep[8] = {0};
     block_segment(ep, s.block, 0xFFFFFFFFu, channels);
     if (channels == 3) {
         ep[3] = 255.0f;
@@ -483,7 +483,7 @@ void bc7_enc_mode6(BC7& s) {
     int32_t qep[8] = {0};
     ep_quant_dequant(qep, ep, mode, channels);
     uint32_t qblock[2] = {0, 0};
-    float err = block_quant(qblock, s.block, bits, ep, 0, channels);
+    real err = block_quant(qblock, s.block, bits, ep, 0, channels);
     uint32_t refine_iterations = s.settings->refine_iterations[mode];
     for (uint32_t it = 0; it < refine_iterations; it++) {
         opt_endpoints(ep, s.block, bits, qblock, 0xFFFFFFFFu, channels);
@@ -499,12 +499,12 @@ void bc7_enc_mode6(BC7& s) {
 // bc7.rs:819-851
 void bc7_enc_mode7(BC7& s) {
     if (s.settings->fast_skip_threshold_mode7 == 0) return;
-    float full_stats[15] = {0};
+    real full_stats[15] = {0};
     compute_stats_masked(full_stats, s.block, 0xFFFFFFFFu, s.settings->channels);
     int32_t part_list[64];
     for (int32_t part = 0; part < 64; part++) {
         uint32_t mask = get_pattern_mask(part, 0);
-        float bound12 = block_pca_bound_split(s.block, mask, full_stats, s.settings->channels);
+        real bound12 = block_pca_bound_split(s.block, mask, full_stats, s.settings->channels);
         int32_t bound = f2i(bound12);
         part_list[part] = part + bound * 64;
     }
@@ -516,7 +516,7 @@ void bc7_enc_mode7(BC7& s) {
 
 // bc7.rs:853-879 (compress_block_bc7_core + compute_opaque_err), fed by the
 // planar block of load_block_interleaved_rgba (bc7.rs:38-63).
-void bc7_encode_block(const float block[64], const BC7Settings* settings, uint32_t out[4]) {
+void bc7_encode_block(const real block[64], const BC7Settings* settings, uint32_t out[4]) {
     BC7 s;
     std::memcpy(s.block, block, sizeof(s.block));
     std::memset(s.data, 0, sizeof(s.data));
@@ -525,7 +525,7 @@ void bc7_encode_block(const float block[64], const BC7Settings* settings, uint32
     if (settings->channels == 3) {
         s.opaque_err = 0.0f;
     } else {
-        float err = 0.0f;
+        real err = 0.0f;
         for (int k = 0; k < 16; k++) err += sq(s.block[48 + k] - 255.0f);
         s.opaque_err = err;
     }

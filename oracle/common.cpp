@@ -78,23 +78,23 @@ void partial_sort_list(int32_t* list, uint32_t length, uint32_t partial_count) {
 }
 
 // common.rs:142-205
-void opt_endpoints(float* ep, const float block[64], uint32_t bits, const uint32_t qblock[2],
+void opt_endpoints(real* ep, const real block[64], uint32_t bits, const uint32_t qblock[2],
                    uint32_t mask, uint32_t channels) {
     int32_t levels = 1 << bits;
-    float atb1[4] = {0, 0, 0, 0};
-    float sum_q = 0.0f;
-    float sum_qq = 0.0f;
-    float sum[5] = {0, 0, 0, 0, 0};
+    real atb1[4] = {0, 0, 0, 0};
+    real sum_q = 0.0f;
+    real sum_qq = 0.0f;
+    real sum[5] = {0, 0, 0, 0, 0};
     uint32_t mask_shifted = mask << 1;
     for (int k1 = 0; k1 < 2; k1++) {
         uint32_t qbits_shifted = qblock[k1];
         for (int k2 = 0; k2 < 8; k2++) {
             int k = k1 * 8 + k2;
-            float q = (float)(qbits_shifted & 15);
+            real q = (real)(qbits_shifted & 15);
             qbits_shifted >>= 4;
             mask_shifted >>= 1;
             if ((mask_shifted & 1) == 0) continue;
-            float x = (float)(levels - 1) - q;
+            real x = (real)(levels - 1) - q;
             sum_q += q;
             sum_qq += q * q;
             sum[4] += 1.0f;
@@ -104,19 +104,19 @@ void opt_endpoints(float* ep, const float block[64], uint32_t bits, const uint32
             }
         }
     }
-    float atb2[4] = {0, 0, 0, 0};
-    for (uint32_t p = 0; p < channels; p++) atb2[p] = (float)(levels - 1) * sum[p] - atb1[p];
+    real atb2[4] = {0, 0, 0, 0};
+    for (uint32_t p = 0; p < channels; p++) atb2[p] = (real)(levels - 1) * sum[p] - atb1[p];
 
-    float lm1 = (float)(levels - 1);
-    float cxx = sum[4] * sq(lm1) - 2.0f * lm1 * sum_q + sum_qq;
-    float cyy = sum_qq;
-    float cxy = lm1 * sum_q - sum_qq;
-    float scale = lm1 / (cxx * cyy - cxy * cxy);
+    real lm1 = (real)(levels - 1);
+    real cxx = sum[4] * sq(lm1) - 2.0f * lm1 * sum_q + sum_qq;
+    real cyy = sum_qq;
+    real cxy = lm1 * sum_q - sum_qq;
+    real scale = lm1 / (cxx * cyy - cxy * cxy);
     for (uint32_t p = 0; p < channels; p++) {
         ep[p] = (atb1[p] * cyy - atb2[p] * cxy) * scale;
         ep[4 + p] = (atb2[p] * cxx - atb1[p] * cxy) * scale;
     }
-    if (std::fabs(cxx * cyy - cxy * cxy) < 0.001f) {
+    if (fabs_r(cxx * cyy - cxy * cxy) < 0.001f) {
         for (uint32_t p = 0; p < channels; p++) {
             ep[p] = sum[p] / sum[4];
             ep[4 + p] = ep[p];
@@ -124,13 +124,13 @@ void opt_endpoints(float* ep, const float block[64], uint32_t bits, const uint32
     }
 }
 
-static void ssymv3(float a[4], const float covar[10], const float b[4]) {
+static void ssymv3(real a[4], const real covar[10], const real b[4]) {
     a[0] = covar[0] * b[0] + covar[1] * b[1] + covar[2] * b[2];
     a[1] = covar[1] * b[0] + covar[4] * b[1] + covar[5] * b[2];
     a[2] = covar[2] * b[0] + covar[5] * b[1] + covar[7] * b[2];
 }
 
-static void ssymv4(float a[4], const float covar[10], const float b[4]) {
+static void ssymv4(real a[4], const real covar[10], const real b[4]) {
     a[0] = covar[0] * b[0] + covar[1] * b[1] + covar[2] * b[2] + covar[3] * b[3];
     a[1] = covar[1] * b[0] + covar[4] * b[1] + covar[5] * b[2] + covar[6] * b[3];
     a[2] = covar[2] * b[0] + covar[5] * b[1] + covar[7] * b[2] + covar[8] * b[3];
@@ -138,17 +138,17 @@ static void ssymv4(float a[4], const float covar[10], const float b[4]) {
 }
 
 // common.rs:260-292
-void compute_axis(float axis[4], const float covar[10], uint32_t power_iterations,
+void compute_axis(real axis[4], const real covar[10], uint32_t power_iterations,
                   uint32_t channels) {
-    float a_vec[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+    real a_vec[4] = {1.0f, 1.0f, 1.0f, 1.0f};
     for (uint32_t i = 0; i < power_iterations; i++) {
         if (channels == 3) ssymv3(axis, covar, a_vec);
         else if (channels == 4) ssymv4(axis, covar, a_vec);
         for (uint32_t p = 0; p < channels; p++) a_vec[p] = axis[p];
         if (i % 2 == 1) {
-            float norm_sq = 0.0f;
+            real norm_sq = 0.0f;
             for (uint32_t p = 0; p < channels; p++) norm_sq += sq(axis[p]);
-            float rnorm = 1.0f / std::sqrt(norm_sq);
+            real rnorm = 1.0f / sqrt_r(norm_sq);
             for (uint32_t p = 0; p < channels; p++) a_vec[p] *= rnorm;
         }
     }
@@ -156,37 +156,37 @@ void compute_axis(float axis[4], const float covar[10], uint32_t power_iteration
 }
 
 // common.rs:208-245
-float get_pca_bound(const float covar[10], uint32_t channels) {
+real get_pca_bound(const real covar[10], uint32_t channels) {
     const uint32_t power_iterations = 4;
-    float cs[10];
-    const float inv_var = 1.0f / (256.0f * 256.0f);
+    real cs[10];
+    const real inv_var = 1.0f / (256.0f * 256.0f);
     for (int i = 0; i < 10; i++) cs[i] = covar[i] * inv_var;
-    const float eps = sq(0.001f);
+    const real eps = sq(0.001f);
     cs[0] += eps;
     cs[4] += eps;
     cs[7] += eps;
-    float axis[4] = {0, 0, 0, 0};
+    real axis[4] = {0, 0, 0, 0};
     compute_axis(axis, cs, power_iterations, channels);
-    float a_vec[4] = {0, 0, 0, 0};
+    real a_vec[4] = {0, 0, 0, 0};
     if (channels == 3) ssymv3(a_vec, cs, axis);
     else if (channels == 4) ssymv4(a_vec, cs, axis);
-    float sq_sum = 0.0f;
+    real sq_sum = 0.0f;
     for (uint32_t p = 0; p < channels; p++) sq_sum += sq(a_vec[p]);
-    float lambda = std::sqrt(sq_sum);
-    float bound = cs[0] + cs[4] + cs[7];
+    real lambda = sqrt_r(sq_sum);
+    real bound = cs[0] + cs[4] + cs[7];
     if (channels == 4) bound += cs[9];
     bound -= lambda;
     return fmax_r(bound, 0.0f);
 }
 
 // common.rs:294-332
-void compute_stats_masked(float stats[15], const float block[64], uint32_t mask,
+void compute_stats_masked(real stats[15], const real block[64], uint32_t mask,
                           uint32_t channels) {
     uint32_t mask_shifted = mask << 1;
     for (int k = 0; k < 16; k++) {
         mask_shifted >>= 1;
-        float flag = (float)(mask_shifted & 1);
-        float rgba[4] = {0, 0, 0, 0};
+        real flag = (real)(mask_shifted & 1);
+        real rgba[4] = {0, 0, 0, 0};
         for (uint32_t p = 0; p < channels; p++) rgba[p] = block[k + p * 16] * flag;
         stats[14] += flag;
         stats[10] += rgba[0];
@@ -209,7 +209,7 @@ void compute_stats_masked(float stats[15], const float block[64], uint32_t mask,
 }
 
 // common.rs:334-350
-void covar_from_stats(float covar[10], const float stats[15], uint32_t channels) {
+void covar_from_stats(real covar[10], const real stats[15], uint32_t channels) {
     covar[0] = stats[0] - stats[10] * stats[10] / stats[14];
     covar[1] = stats[1] - stats[10] * stats[11] / stats[14];
     covar[2] = stats[2] - stats[10] * stats[12] / stats[14];
@@ -225,23 +225,23 @@ void covar_from_stats(float covar[10], const float stats[15], uint32_t channels)
 }
 
 // common.rs:352-368
-void compute_covar_dc_masked(float covar[10], float dc[4], const float block[64], uint32_t mask,
+void compute_covar_dc_masked(real covar[10], real dc[4], const real block[64], uint32_t mask,
                              uint32_t channels) {
-    float stats[15] = {0};
+    real stats[15] = {0};
     compute_stats_masked(stats, block, mask, channels);
     for (uint32_t p = 0; p < channels; p++) dc[p] = stats[10 + p] / stats[14];
     covar_from_stats(covar, stats, channels);
 }
 
 // common.rs:370-394
-void block_pca_axis(float axis[4], float dc[4], const float block[64], uint32_t mask,
+void block_pca_axis(real axis[4], real dc[4], const real block[64], uint32_t mask,
                     uint32_t channels) {
     const uint32_t power_iterations = 8;
-    float covar[10] = {0};
+    real covar[10] = {0};
     compute_covar_dc_masked(covar, dc, block, mask, channels);
-    const float inv_var = 1.0f / (256.0f * 256.0f);
+    const real inv_var = 1.0f / (256.0f * 256.0f);
     for (int i = 0; i < 10; i++) covar[i] *= inv_var;
-    const float eps = sq(0.001f);
+    const real eps = sq(0.001f);
     covar[0] += eps;
     covar[4] += eps;
     covar[7] += eps;
@@ -250,25 +250,25 @@ void block_pca_axis(float axis[4], float dc[4], const float block[64], uint32_t 
 }
 
 // common.rs:396-420
-float block_pca_bound_split(const float block[64], uint32_t mask, const float full_stats[15],
+real block_pca_bound_split(const real block[64], uint32_t mask, const real full_stats[15],
                             uint32_t channels) {
-    float stats[15] = {0};
+    real stats[15] = {0};
     compute_stats_masked(stats, block, mask, channels);
-    float covar1[10] = {0};
+    real covar1[10] = {0};
     covar_from_stats(covar1, stats, channels);
     for (int i = 0; i < 15; i++) stats[i] = full_stats[i] - stats[i];
-    float covar2[10] = {0};
+    real covar2[10] = {0};
     covar_from_stats(covar2, stats, channels);
-    float bound = 0.0f;
+    real bound = 0.0f;
     bound += get_pca_bound(covar1, channels);
     bound += get_pca_bound(covar2, channels);
-    return std::sqrt(bound) * 256.0f;
+    return sqrt_r(bound) * 256.0f;
 }
 
 // common.rs:422-481
-float block_quant(uint32_t qblock[2], const float block[64], uint32_t bits, const float* ep,
+real block_quant(uint32_t qblock[2], const real block[64], uint32_t bits, const real* ep,
                   uint32_t pattern, uint32_t channels) {
-    float total_err = 0.0f;
+    real total_err = 0.0f;
     int32_t levels = 1 << bits;
     qblock[0] = 0;
     qblock[1] = 0;
@@ -276,30 +276,30 @@ float block_quant(uint32_t qblock[2], const float block[64], uint32_t bits, cons
     for (int k = 0; k < 16; k++) {
         uint32_t j = pattern_shifted & 3;
         pattern_shifted >>= 2;
-        float proj = 0.0f;
-        float div = 0.0f;
+        real proj = 0.0f;
+        real div = 0.0f;
         for (uint32_t p = 0; p < channels; p++) {
-            float ep_a = ep[8 * j + p];
-            float ep_b = ep[8 * j + 4 + p];
+            real ep_a = ep[8 * j + p];
+            real ep_b = ep[8 * j + 4 + p];
             proj += (block[k + p * 16] - ep_a) * (ep_b - ep_a);
             div += sq(ep_b - ep_a);
         }
         proj /= div;
-        int32_t q1 = f2i(proj * (float)levels + 0.5f);
+        int32_t q1 = f2i(proj * (real)levels + 0.5f);
         int32_t q1_clamped = clampi_r(q1, 1, levels - 1);
-        float err0 = 0.0f;
-        float err1 = 0.0f;
+        real err0 = 0.0f;
+        real err1 = 0.0f;
         int32_t w0 = get_unquant_value(bits, q1_clamped - 1);
         int32_t w1 = get_unquant_value(bits, q1_clamped);
         for (uint32_t p = 0; p < channels; p++) {
-            float ep_a = ep[8 * j + p];
-            float ep_b = ep[8 * j + 4 + p];
-            float dec_v0 = (float)(((64 - w0) * f2i(ep_a) + w0 * f2i(ep_b) + 32) / 64);
-            float dec_v1 = (float)(((64 - w1) * f2i(ep_a) + w1 * f2i(ep_b) + 32) / 64);
+            real ep_a = ep[8 * j + p];
+            real ep_b = ep[8 * j + 4 + p];
+            real dec_v0 = (real)(((64 - w0) * f2i(ep_a) + w0 * f2i(ep_b) + 32) / 64);
+            real dec_v1 = (real)(((64 - w1) * f2i(ep_a) + w1 * f2i(ep_b) + 32) / 64);
             err0 += sq(dec_v0 - block[k + p * 16]);
             err1 += sq(dec_v1 - block[k + p * 16]);
         }
-        float best_err = err1;
+        real best_err = err1;
         int32_t best_q = q1_clamped;
         if (err0 < err1) {
             best_err = err0;
@@ -312,16 +312,16 @@ float block_quant(uint32_t qblock[2], const float block[64], uint32_t bits, cons
 }
 
 // common.rs:483-518
-void block_segment_core(float* ep, const float block[64], uint32_t mask, uint32_t channels) {
-    float axis[4] = {0, 0, 0, 0};
-    float dc[4] = {0, 0, 0, 0};
+void block_segment_core(real* ep, const real block[64], uint32_t mask, uint32_t channels) {
+    real axis[4] = {0, 0, 0, 0};
+    real dc[4] = {0, 0, 0, 0};
     block_pca_axis(axis, dc, block, mask, channels);
-    float ext[2] = {INFINITY, -INFINITY};
+    real ext[2] = {INFINITY, -INFINITY};
     uint32_t mask_shifted = mask << 1;
     for (int k = 0; k < 16; k++) {
         mask_shifted >>= 1;
         if ((mask_shifted & 1) == 0) continue;
-        float dot = 0.0f;
+        real dot = 0.0f;
         for (uint32_t p = 0; p < channels; p++) dot += axis[p] * (block[16 * p + k] - dc[p]);
         ext[0] = fmin_r(ext[0], dot);
         ext[1] = fmax_r(ext[1], dot);

@@ -63,6 +63,19 @@ inline uint32_t clampu_r(uint32_t x, uint32_t lo, uint32_t hi) {
 
 inline float sq(float x) { return x * x; }
 
+// The encoder sources compute in `real`: plain f32 here, an op-counting f32
+// in the op-counting build (oracle_count.h, -DORACLE_COUNT_OPS) that measures
+// the reference algorithm's arithmetic per block.
+#ifdef ORACLE_COUNT_OPS
+}  // namespace oracle
+#include "oracle_count.h"
+namespace oracle {
+#else
+using real = float;
+inline float sqrt_r(float x) { return std::sqrt(x); }
+inline float fabs_r(float x) { return std::fabs(x); }
+#endif
+
 // Settings structs: byte layout of the reference's #[repr(C)] structs
 // (src/settings.rs:207-213 and :278-288).
 struct BC6HSettings {
@@ -94,23 +107,23 @@ void get_skips(int32_t part_id, uint32_t skips[3]);                 // common.rs
 void put_bits(uint32_t data[5], uint32_t* pos, uint32_t bits, uint32_t v);  // common.rs:103
 void data_shl_1bit_from(uint32_t data[5], uint32_t from_bits);      // common.rs:111
 void partial_sort_list(int32_t* list, uint32_t length, uint32_t partial_count);  // :126
-void opt_endpoints(float* ep, const float block[64], uint32_t bits, const uint32_t qblock[2],
+void opt_endpoints(real* ep, const real block[64], uint32_t bits, const uint32_t qblock[2],
                    uint32_t mask, uint32_t channels);               // common.rs:142
-float get_pca_bound(const float covar[10], uint32_t channels);      // common.rs:208
-void compute_axis(float axis[4], const float covar[10], uint32_t power_iterations,
+real get_pca_bound(const real covar[10], uint32_t channels);      // common.rs:208
+void compute_axis(real axis[4], const real covar[10], uint32_t power_iterations,
                   uint32_t channels);                               // common.rs:260
-void compute_stats_masked(float stats[15], const float block[64], uint32_t mask,
+void compute_stats_masked(real stats[15], const real block[64], uint32_t mask,
                           uint32_t channels);                       // common.rs:294
-void covar_from_stats(float covar[10], const float stats[15], uint32_t channels);  // :334
-void compute_covar_dc_masked(float covar[10], float dc[4], const float block[64], uint32_t mask,
+void covar_from_stats(real covar[10], const real stats[15], uint32_t channels);  // :334
+void compute_covar_dc_masked(real covar[10], real dc[4], const real block[64], uint32_t mask,
                              uint32_t channels);                    // common.rs:352
-void block_pca_axis(float axis[4], float dc[4], const float block[64], uint32_t mask,
+void block_pca_axis(real axis[4], real dc[4], const real block[64], uint32_t mask,
                     uint32_t channels);                             // common.rs:370
-float block_pca_bound_split(const float block[64], uint32_t mask, const float full_stats[15],
+real block_pca_bound_split(const real block[64], uint32_t mask, const real full_stats[15],
                             uint32_t channels);                     // common.rs:396
-float block_quant(uint32_t qblock[2], const float block[64], uint32_t bits, const float* ep,
+real block_quant(uint32_t qblock[2], const real block[64], uint32_t bits, const real* ep,
                   uint32_t pattern, uint32_t channels);             // common.rs:422
-void block_segment_core(float* ep, const float block[64], uint32_t mask, uint32_t channels);
+void block_segment_core(real* ep, const real block[64], uint32_t mask, uint32_t channels);
 void bc7_code_qblock(uint32_t data[5], uint32_t* qpos, const uint32_t qblock[2], uint32_t bits,
                      uint32_t flips);                               // common.rs:520
 void bc7_code_adjust_skip_mode01237(uint32_t data[5], uint32_t mode, int32_t part_id);
@@ -123,11 +136,11 @@ uint32_t bc7_code_apply_swap_mode01237(int32_t qep[24], const uint32_t qblock[2]
 
 // BC1-BC5 (src/encode/bc1_to_5.rs). `block` is the planar f32[64] layout
 // R=0..15, G=16..31, B=32..47, A=48..63.
-void bc1_core(const float block[64], uint32_t out[2]);       // bc1_to_5.rs:386
-void bc3_alpha(const float block[64], uint32_t out[2]);      // bc1_to_5.rs:431
+void bc1_core(const real block[64], uint32_t out[2]);       // bc1_to_5.rs:386
+void bc3_alpha(const real block[64], uint32_t out[2]);      // bc1_to_5.rs:431
 
 // BC7 (src/encode/bc7.rs) and BC6H (src/encode/bc6h.rs).
-void bc7_encode_block(const float block[64], const BC7Settings* s, uint32_t out[4]);
-void bc6h_encode_block(const float block_in[64], const BC6HSettings* s, uint32_t out[4]);
+void bc7_encode_block(const real block[64], const BC7Settings* s, uint32_t out[4]);
+void bc6h_encode_block(const real block_in[64], const BC6HSettings* s, uint32_t out[4]);
 
 }  // namespace oracle
