@@ -374,6 +374,77 @@ def profile_case(args):
     print(json.dumps({"case": args.case, "ms": ms, "mpx_s": size * size / ms / 1e3}), flush=True)
 
 
+def batched_mips_bench(args):
+    """Batched mixed workload: 64 RGBA8 textures with sides drawn from
+    {16, 20, ..., 4096}, each with its full box-filtered mip chain (GPU), BC1 /
+    BC5 / BC7 alpha_basic round-robin; the per-task path (one launch sequence
+    per texture level) against the batched CUDA graph with the autotuned
+    launch shape. Prints one line (not the benchmark contract line)."""
+    import torch
+
+    import block_compression_b200 as bcn
+    from block_compression_b200 import mips, synthetic
+
+    dev = torch.device("cuda", 0)
+    V = bcn.CompressionVariant
+    variants = [V.BC1, V.BC5, V.BC7(bcn.BC7Settings.alpha_basic())]
+    shapes = synthetic.config4_textures(seed=4, count=args.textures)
+    chains = [mips.generate_mip_chain(synthetic.rgba8_textured_torch(4000 + i, h, w, dev)) for i, (h, w) in
+              enumerate(shapes)]
+    torch.cuda.synchronize()
+    tasks, total, px = [], 0, 0
+    for i, chain in enumerate(chains):
+        v = variants[i % 3]
+        for lv in chain:
+            n = v.blocks_byte_size(lv.padded_width, lv.padded_height)
+            tasks.append((lv, v, total))
+            total += n
+            px += lv.padded_width * lv.padded_height
+    out_plain = torch.zeros(total, dtype=torch.uint8, device=dev)
+    out_batch = torch.zeros(total, dtype=torch.uint8, device=dev)
+
+    def add(c, out):
+        for lv, v, off in tasks:
+            c.add_compression_task(v, lv.data, lv.padded_width, lv.padded_height, out, blocks_offset=off)
+
+    c = bcn.GpuBlockCompressor()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    plain_ms = []
+    for i in range(args.warmup + args.steps):
+        add(c, out_plain)
+        a, b = ev(), ev()
+        a.record()
+        c.compress()
+        b.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            plain_ms.append(a.elapsed_time(b))
+    add(c, out_batch)
+    t0 = time.perf_counter()
+    batch = c.create_batch(autotune=True)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    batch_ms = []
+    for i in range(args.warmup + args.steps):
+        a, b = ev(), ev()
+        a.record()
+        batch.launch()
+        b.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            batch_ms.append(a.elapsed_time(b))
+    same = bool(torch.equal(out_plain, out_batch))
+    pm, bm = sum(plain_ms) / len(plain_ms), sum(batch_ms) / len(batch_ms)
+    print(json.dumps({
+        "workload": "%d RGBA8 textures, sides in {16..4096}, full mip chains, BC1/BC5/BC7 alpha_basic round-robin"
+                    % args.textures,
+        "tasks": len(tasks), "encoded_mpx": px / 1e6, "plain_ms": pm, "batched_ms": bm,
+        "plain_mpx_s": px / pm / 1e3, "batched_mpx_s": px / bm / 1e3, "batched_over_plain": pm / bm,
+        "tune": batch.tune.as_dict(), "autotune_s": tune_s, "outputs_identical": same,
+    }), flush=True)
+    batch.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,10 +453,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--case", default=None, help="profiling case VARIANT:SIZE, e.g. bc7:512 (not a bench line)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "mips"],
+                    help="c2: the benchmark line; mips: batched mixed mip-chain workload (extra line)")
+    ap.add_argument("--textures", type=int, default=64)
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.case:
         profile_case(args)
+    elif args.workload == "mips":
+        batched_mips_bench(args)
     elif args.impl == "reference":
         cpu_reference(args, world, rank)
     else:

@@ -8,12 +8,12 @@ hand-written sm_100a kernels in libbcn_b200.so behind a C ABI
 the library is missing.
 """
 from ._lib import BcError, lib  # noqa: F401  (loads libbcn_b200.so or raises)
-from .compressor import GpuBlockCompressor
+from .compressor import Batch, GpuBlockCompressor, Tune
 from .settings import BC6HSettings, BC7Settings, CompressionVariant
 from . import decode, encode
 
-__all__ = ["BC6HSettings", "BC7Settings", "CompressionVariant", "GpuBlockCompressor", "BcError", "encode", "decode",
-           "version"]
+__all__ = ["BC6HSettings", "BC7Settings", "CompressionVariant", "GpuBlockCompressor", "Batch", "Tune", "BcError",
+           "encode", "decode", "version"]
 
 
 def version():

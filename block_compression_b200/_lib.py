@@ -60,6 +60,13 @@ def _load():
         "bc_compressor_add_task": ([P, I, P, P, S, S, U32, U32, U32, P, S, U32], I),
         "bc_compressor_compress": ([P, P], I),
         "bc_compressor_task_count": ([P], I),
+        "bc_batch_create": ([P, P, I, P, ctypes.POINTER(P)], I),
+        "bc_batch_launch": ([P, P], I),
+        "bc_batch_get_tune": ([P, P], I),
+        "bc_batch_destroy": ([P], I),
+        "bc_compressor_compress_batched": ([P, P, P], I),
+        "bc_compress_bc7_device_noalloc": ([P, P, S, P, S, U32, U32, S, P], I),
+        "bc_mip_level_rgba8_device": ([P, S, U32, U32, P, S, S, P], I),
         "bc_last_cuda_error": ([], I),
         "bc_version": ([], ctypes.c_char_p),
     }

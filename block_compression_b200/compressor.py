@@ -68,3 +68,68 @@ class GpuBlockCompressor:
             self.close()
         except Exception:
             pass
+
+
+class Tune(ctypes.Structure):
+    """Launch shape of a batch (include/bc_capi.h, bc_tune)."""
+
+    _fields_ = [("threads_per_cta", ctypes.c_uint32), ("ctas_per_sm", ctypes.c_uint32),
+                ("tiles_per_claim", ctypes.c_uint32), ("bc7_search_warps", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Batch:
+    """Every pending task of a GpuBlockCompressor frozen into one device task
+    table and one CUDA graph (bc_batch). launch() replays it."""
+
+    def __init__(self, compressor, tune=None, autotune=True, stream=None):
+        s = stream if stream is not None else _buffers.current_stream_ptr()
+        h = ctypes.c_void_p()
+        tp = ctypes.byref(tune) if tune is not None else None
+        check("bc_batch_create", lib.bc_batch_create(compressor._h, tp, int(bool(autotune)), s, ctypes.byref(h)))
+        self._h = h
+        self._keep = list(compressor._keep)  # the tasks' buffers must outlive the batch
+        compressor._keep.clear()
+
+    def launch(self, stream=None):
+        s = stream if stream is not None else _buffers.current_stream_ptr()
+        check("bc_batch_launch", lib.bc_batch_launch(self._h, s))
+
+    @property
+    def tune(self):
+        t = Tune()
+        check("bc_batch_get_tune", lib.bc_batch_get_tune(self._h, ctypes.byref(t)))
+        return t
+
+    def close(self):
+        if self._h:
+            lib.bc_batch_destroy(self._h)
+            self._h = None
+            self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _compress_batched(self, stream=None, tune=None):
+    """All pending tasks in one batched graph launch (autotuned unless `tune`
+    is given); synchronises the stream before returning."""
+    s = stream if stream is not None else _buffers.current_stream_ptr()
+    tp = ctypes.byref(tune) if tune is not None else None
+    try:
+        check("bc_compressor_compress_batched", lib.bc_compressor_compress_batched(self._h, s, tp))
+    finally:
+        self._keep.clear()
+
+
+def _create_batch(self, tune=None, autotune=True, stream=None):
+    return Batch(self, tune=tune, autotune=autotune, stream=stream)
+
+
+GpuBlockCompressor.compress_batched = _compress_batched
+GpuBlockCompressor.create_batch = _create_batch

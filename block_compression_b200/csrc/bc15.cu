@@ -436,6 +436,61 @@ __global__ void __launch_bounds__(128) bc15_decode_kernel(const uint8_t* __restr
     }
 }
 
+// ---- batched: persistent work-queue kernel ---------------------------------------
+//
+// One launch encodes the tiles (32 blocks) of many BC1-BC5 regions of mixed
+// variants. CTAs stay resident and claim work from a global counter: each
+// claim hands NWARP*tiles_per_claim consecutive tiles to the CTA, warp w
+// takes tiles base + i*NWARP + w. The loop ends when a claim starts past the
+// last tile, so it runs at most ntiles / (NWARP*tiles_per_claim) + 1 times
+// per CTA (no waiting on other CTAs).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) bc15_batch_kernel(const TaskDesc* __restrict__ tasks,
+                                                              const uint32_t* __restrict__ tile_task, uint32_t ntiles,
+                                                              uint32_t* counter, int tiles_per_claim) {
+    constexpr int NWARP = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ uint32_t base_s;
+    for (;;) {
+        if (threadIdx.x == 0) base_s = atomicAdd(counter, (uint32_t)(NWARP * tiles_per_claim));
+        __syncthreads();
+        const uint32_t base = base_s;
+        __syncthreads();
+        if (base >= ntiles) break;
+        for (int i = 0; i < tiles_per_claim; i++) {
+            const uint32_t tile = base + (uint32_t)(i * NWARP + warp);
+            if (tile >= ntiles) break;
+            const TaskDesc d = tasks[tile_task[tile]];
+            const uint32_t lb = (tile - d.tile_base) * 32 + lane;
+            if (lb >= d.bw * d.bh) continue;
+            const uint32_t by = lb / d.bw, bx = lb - by * d.bw;
+            Px16 px;
+            if (d.aligned) load_rgba8<true>(d.src, d.stride, bx, by, px);
+            else load_rgba8<false>(d.src, d.stride, bx, by, px);
+            uint32_t w[4];
+            encode_bc15_block((int)d.variant, px, w);
+            const int words = (d.variant == BC_BC1 || d.variant == BC_BC4) ? 2 : 4;
+            uint8_t* o = d.dst + (size_t)lb * (words * 4);
+            if (((uintptr_t)o & (words * 4 - 1)) == 0) {
+                if (words == 2) *reinterpret_cast<uint2*>(o) = make_uint2(w[0], w[1]);
+                else *reinterpret_cast<uint4*>(o) = make_uint4(w[0], w[1], w[2], w[3]);
+            } else {
+                for (int j = 0; j < words; j++) reinterpret_cast<uint32_t*>(o)[j] = w[j];
+            }
+        }
+    }
+}
+
+cudaError_t launch_bc15_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
+                              uint32_t* counter_dev, int threads, int ctas, int tiles_per_claim, cudaStream_t s) {
+    if (ntiles == 0) return cudaSuccess;
+    if (tiles_per_claim < 1) tiles_per_claim = 1;
+    if (threads == 256) bc15_batch_kernel<256><<<ctas, 256, 0, s>>>(tasks_dev, tile_task_dev, ntiles, counter_dev,
+                                                                   tiles_per_claim);
+    else bc15_batch_kernel<128><<<ctas, 128, 0, s>>>(tasks_dev, tile_task_dev, ntiles, counter_dev, tiles_per_claim);
+    return cudaGetLastError();
+}
+
 // ---- launchers ------------------------------------------------------------------
 
 static int grid_for(uint32_t n, int threads) {

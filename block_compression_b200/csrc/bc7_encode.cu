@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <cstring>
 
 #include "bc_common.cuh"
 #include "bc_kernels.h"
@@ -455,13 +456,17 @@ static __host__ __device__ Plan make_plan(const BC7SettingsDev& s) {
 }
 
 // Arguments shared by every kernel of one encode. Scratch arrays are indexed
-// [row * npad + block] so a warp's 32 lanes touch 32 consecutive entries.
+// [row * npad + tile * 32 + lane] so a warp's 32 lanes touch 32 consecutive
+// entries. A single-image encode describes its image inline; a batched
+// encode (tasks != nullptr) maps every global tile to the task it belongs to.
 struct Work {
     const uint8_t* src;
     size_t stride;
     uint32_t bw, nblocks, npad;
     bool aligned;
     uint8_t* dst;
+    const TaskDesc* tasks;     // batched encodes only
+    const uint32_t* tile_task; // batched encodes only: task index of each tile
     uint8_t* lists;            // [row * npad + block]: rows 0..k_a-1 list A, then k_b rows of list B
     unsigned long long* keys;  // [mi * npad + block]: (error bits << 32) | candidate
     float* slot_err;           // [slot * npad + block]
@@ -469,18 +474,54 @@ struct Work {
     BC7SettingsDev S;
 };
 
+// Where the tile's blocks come from and go to.
+struct TileLoc {
+    const uint8_t* src;
+    size_t stride;
+    uint8_t* dst;
+    uint32_t bw;
+    uint32_t first;    // block index (within its image) of the tile's lane 0
+    uint32_t nblocks;  // blocks of its image
+    bool aligned;
+    BCN_DEV bool valid(int lane) const { return first + lane < nblocks; }
+};
+
+BCN_DEV TileLoc tile_loc(const Work& w, uint32_t tile) {
+    TileLoc t;
+    if (w.tasks == nullptr) {
+        t.src = w.src;
+        t.stride = w.stride;
+        t.dst = w.dst;
+        t.bw = w.bw;
+        t.first = tile * NB;
+        t.nblocks = w.nblocks;
+        t.aligned = w.aligned;
+    } else {
+        const TaskDesc& d = w.tasks[w.tile_task[tile]];
+        t.src = d.src;
+        t.stride = d.stride;
+        t.dst = d.dst;
+        t.bw = d.bw;
+        t.first = (tile - d.tile_base) * NB;
+        t.nblocks = d.bw * d.bh;
+        t.aligned = d.aligned != 0;
+    }
+    return t;
+}
+
 // Stages the 32 blocks of `tile` into px (planar f32, lane-strided) with
 // threads tid = 0..nt-1 (128-bit loads: the 4 rows of 32 neighbouring blocks
 // are 4 contiguous 512-byte spans).
 BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, int nt) {
+    const TileLoc L = tile_loc(w, tile);
     for (int t = tid; t < NB * 4; t += nt) {
         int b = t & 31, y = t >> 5;
-        uint32_t gi = tile * NB + b;
+        uint32_t gi = L.first + b;
         uint32_t v[4] = {0, 0, 0, 0};
-        if (gi < w.nblocks) {
-            uint32_t by = gi / w.bw, bx = gi - by * w.bw;
-            const uint8_t* row = w.src + (size_t)(by * 4 + y) * w.stride + (size_t)bx * 16;
-            if (w.aligned) {
+        if (gi < L.nblocks) {
+            uint32_t by = gi / L.bw, bx = gi - by * L.bw;
+            const uint8_t* row = L.src + (size_t)(by * 4 + y) * L.stride + (size_t)bx * 16;
+            if (L.aligned) {
                 uint4 q = __ldg(reinterpret_cast<const uint4*>(row));
                 v[0] = q.x;
                 v[1] = q.y;
@@ -584,7 +625,7 @@ __global__ void __launch_bounds__(NW * 32) bc7_search_kernel(Work w) {
     __syncthreads();
     const int c = blockIdx.y * NW + warp;
     unsigned long long key = ~0ull;
-    if (c < P.count[mi] && gi < w.nblocks) {
+    if (c < P.count[mi] && tile_loc(w, tile).valid(lane)) {
         const Blk blk{&px[0][lane]};
         int qep[24];
         uint32_t q0, q1;
@@ -617,7 +658,7 @@ __global__ void __launch_bounds__(NW * 32) bc7_refine_kernel(Work w, uint32_t nt
     unsigned long long key = w.keys[(size_t)mi * w.npad + gi];
     float err = __int_as_float(0x7f800000);
     uint4 data = make_uint4(0, 0, 0, 0);
-    if (key != ~0ull && gi < w.nblocks) {
+    if (key != ~0ull && tile_loc(w, tile).valid(lane)) {
         int c = (int)(key & 0xFFFFFFFFu);
         float e0 = __uint_as_float((uint32_t)(key >> 32));
         int iters = (int)w.S.refine_iterations[MODE];
@@ -675,9 +716,13 @@ __global__ void __launch_bounds__(NW * 32) bc7_mode6_kernel(Work w, uint32_t nti
 // the best so far, scanning modes 0,2,1,3,7, the mode-4 then mode-5
 // candidates, then mode 6 (bc7.rs:602-609, 735-760, 813-816): the first slot
 // holding the minimum wins. A block no mode encodes stays all-zero.
-__global__ void __launch_bounds__(256) bc7_select_kernel(Work w) {
-    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= w.nblocks) return;
+__global__ void __launch_bounds__(256) bc7_select_kernel(Work w, uint32_t ntiles) {
+    const uint32_t tile = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (tile >= ntiles) return;
+    const TileLoc L = tile_loc(w, tile);
+    if (!L.valid(lane)) return;
+    const uint32_t gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
     float best = __int_as_float(0x7f800000);
     int win = -1;
@@ -706,8 +751,8 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w) {
         }
     }
     uint4 data = win >= 0 ? w.slot_data[(size_t)win * w.npad + gi] : make_uint4(0, 0, 0, 0);
-    uint8_t* o = w.dst + (size_t)gi * 16;
-    if (((uintptr_t)w.dst & 15) == 0) {
+    uint8_t* o = L.dst + (size_t)(L.first + lane) * 16;
+    if (((uintptr_t)L.dst & 15) == 0) {
         *reinterpret_cast<uint4*>(o) = data;
     } else {
         uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
@@ -720,30 +765,26 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w) {
 
 }  // namespace bc7
 
-size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& s) {
+size_t bc7_scratch_bytes_tiles(uint32_t ntiles, const BC7SettingsDev& s) {
     const bc7::Plan P = bc7::make_plan(s);
-    size_t npad = ((size_t)nblocks + bc7::NB - 1) / bc7::NB * bc7::NB;
+    size_t npad = (size_t)ntiles * bc7::NB;
     int nslots = 5 + P.n45_4 + P.n45_5 + 1;
     return npad * ((size_t)(P.k_a + P.k_b) + 5 * 8 + (size_t)nslots * (4 + 16)) + 256;
 }
 
-cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
-                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s) {
-    using namespace bc7;
-    uint32_t n = bw * bh;
-    if (n == 0) return cudaSuccess;
-    const Plan P = make_plan(settings);
-    uint32_t ntiles = (n + NB - 1) / NB;
+size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& s) {
+    return bc7_scratch_bytes_tiles((nblocks + bc7::NB - 1) / bc7::NB, s);
+}
+
+namespace bc7 {
+
+// Carves the scratch arrays out of `scratch` and enqueues the pipeline over
+// `ntiles` tiles.
+static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int search_warps, cudaStream_t s) {
+    const Plan P = make_plan(w.S);
     size_t npad = (size_t)ntiles * NB;
     int nslots = 5 + P.n45_4 + P.n45_5 + 1;
-    Work w;
-    w.src = src;
-    w.stride = stride;
-    w.bw = bw;
-    w.nblocks = n;
     w.npad = (uint32_t)npad;
-    w.aligned = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
-    w.dst = dst;
     uint8_t* p = (uint8_t*)(((uintptr_t)scratch + 255) & ~(uintptr_t)255);
     w.slot_data = (uint4*)p;
     p += npad * 16 * nslots;
@@ -752,16 +793,33 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
     w.slot_err = (float*)p;
     p += npad * 4 * nslots;
     w.lists = p;
-    w.S = settings;
 
-    constexpr int NWP = 8, NWS = 8, NWR = 4, NW45 = 4;
+    constexpr int NWP = 8, NWR = 4, NW45 = 4;
     bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
     auto groups = [](int count, int nw) { return (unsigned)((count + nw - 1) / nw); };
-    if (P.count[0]) bc7_search_kernel<0, NWS><<<dim3(ntiles, groups(P.count[0], NWS)), NWS * 32, 0, s>>>(w);
-    if (P.count[1]) bc7_search_kernel<2, NWS><<<dim3(ntiles, groups(P.count[1], NWS)), NWS * 32, 0, s>>>(w);
-    if (P.count[2]) bc7_search_kernel<1, NWS><<<dim3(ntiles, groups(P.count[2], NWS)), NWS * 32, 0, s>>>(w);
-    if (P.count[3]) bc7_search_kernel<3, NWS><<<dim3(ntiles, groups(P.count[3], NWS)), NWS * 32, 0, s>>>(w);
-    if (P.count[4]) bc7_search_kernel<7, NWS><<<dim3(ntiles, groups(P.count[4], NWS)), NWS * 32, 0, s>>>(w);
+    const int modes[5] = {0, 2, 1, 3, 7};
+    for (int mi = 0; mi < 5; mi++) {
+        if (!P.count[mi]) continue;
+        if (search_warps == 4) {
+            dim3 g(ntiles, groups(P.count[mi], 4));
+            switch (modes[mi]) {
+                case 0: bc7_search_kernel<0, 4><<<g, 128, 0, s>>>(w); break;
+                case 2: bc7_search_kernel<2, 4><<<g, 128, 0, s>>>(w); break;
+                case 1: bc7_search_kernel<1, 4><<<g, 128, 0, s>>>(w); break;
+                case 3: bc7_search_kernel<3, 4><<<g, 128, 0, s>>>(w); break;
+                default: bc7_search_kernel<7, 4><<<g, 128, 0, s>>>(w); break;
+            }
+        } else {
+            dim3 g(ntiles, groups(P.count[mi], 8));
+            switch (modes[mi]) {
+                case 0: bc7_search_kernel<0, 8><<<g, 256, 0, s>>>(w); break;
+                case 2: bc7_search_kernel<2, 8><<<g, 256, 0, s>>>(w); break;
+                case 1: bc7_search_kernel<1, 8><<<g, 256, 0, s>>>(w); break;
+                case 3: bc7_search_kernel<3, 8><<<g, 256, 0, s>>>(w); break;
+                default: bc7_search_kernel<7, 8><<<g, 256, 0, s>>>(w); break;
+            }
+        }
+    }
     unsigned rgrid = (ntiles + NWR - 1) / NWR;
     if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
@@ -770,7 +828,7 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
     if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.n45_5) {
         dim3 g45(ntiles, groups(P.n45_5, NW45));
-        if (settings.channels == 4) {
+        if (w.S.channels == 4) {
             bc7_mode45_kernel<4, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
             bc7_mode45_kernel<4, 1, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
             bc7_mode45_kernel<5, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
@@ -781,11 +839,43 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
         }
     }
     if (P.run6) {
-        if (settings.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+        if (w.S.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
         else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     }
-    bc7_select_kernel<<<(n + 255) / 256, 256, 0, s>>>(w);
+    bc7_select_kernel<<<(ntiles + 7) / 8, 256, 0, s>>>(w, ntiles);
     return cudaGetLastError();
+}
+
+}  // namespace bc7
+
+cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
+                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s) {
+    using namespace bc7;
+    uint32_t n = bw * bh;
+    if (n == 0) return cudaSuccess;
+    Work w;
+    w.src = src;
+    w.stride = stride;
+    w.bw = bw;
+    w.nblocks = n;
+    w.aligned = ((uintptr_t)src % 16 == 0) && (stride % 16 == 0);
+    w.dst = dst;
+    w.tasks = nullptr;
+    w.tile_task = nullptr;
+    w.S = settings;
+    return run_pipeline(w, (n + NB - 1) / NB, scratch, 8, s);
+}
+
+cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
+                             const BC7SettingsDev& settings, void* scratch, int search_warps, cudaStream_t s) {
+    using namespace bc7;
+    if (ntiles == 0) return cudaSuccess;
+    Work w;
+    memset(&w, 0, sizeof(w));
+    w.tasks = tasks_dev;
+    w.tile_task = tile_task_dev;
+    w.S = settings;
+    return run_pipeline(w, ntiles, scratch, search_warps, s);
 }
 
 }  // namespace bcn

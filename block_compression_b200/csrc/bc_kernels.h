@@ -23,6 +23,20 @@ struct BC7SettingsDev {
     uint32_t mode45_channel0, refine_iterations_channel, channels;
 };
 
+// One texture region of a batched launch: blocks of the region are numbered
+// row-major from 0; its tiles of 32 blocks occupy the batch's global tile
+// range [tile_base, tile_base + ceil(bw*bh/32)).
+struct TaskDesc {
+    const uint8_t* src;  // row 0 of the region
+    uint8_t* dst;        // first block of the region
+    uint64_t stride;     // bytes per source row
+    uint32_t bw, bh;     // size in blocks
+    uint32_t tile_base;
+    uint32_t variant;
+    uint32_t aligned;    // src and stride 16-byte aligned
+    uint32_t pad;
+};
+
 // Source pixel formats a BC6H launch can read.
 enum Bc6hSource { BC6H_SRC_RGBA16F = 0, BC6H_SRC_RGBA8_SRGB = 1 };
 
@@ -35,6 +49,17 @@ void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_
 size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& settings);
 cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
                               const BC7SettingsDev& settings, void* scratch, cudaStream_t s);
+// Batched form: the pipeline over `ntiles` tiles of several regions
+// (tasks_dev / tile_task_dev in device memory). search_warps: 4 or 8
+// candidates per CTA in the search launches.
+size_t bc7_scratch_bytes_tiles(uint32_t ntiles, const BC7SettingsDev& settings);
+cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
+                             const BC7SettingsDev& settings, void* scratch, int search_warps, cudaStream_t s);
+// Persistent work-queue kernel over the tiles of BC1-BC5 regions: CTAs claim
+// `tiles_per_claim` tiles per warp from *counter (zeroed by the caller) until
+// the list is exhausted.
+cudaError_t launch_bc15_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
+                              uint32_t* counter_dev, int threads, int ctas, int tiles_per_claim, cudaStream_t s);
 void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s);
 // stride in bytes of the source rows (RGBA16F: 8 bytes per pixel; RGBA8: 4).
 void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,

@@ -559,6 +559,38 @@ extern "C" int bc_compressor_compress(bc_compressor* c, void* stream) {
     return rc;
 }
 
+// Task access for the batched path (batch.cu).
+namespace bcn {
+struct BcTaskView {
+    int variant;
+    const void* settings;
+    const uint8_t* src;
+    size_t pitch;
+    uint32_t w, h;
+    uint8_t* dst;
+};
+int compressor_tasks(bc_compressor* c, std::vector<BcTaskView>& out, int* device) {
+    if (!c) return BC_ERR_TASKS;
+    *device = c->device;
+    out.clear();
+    for (const BcTask& t : c->tasks) {
+        BcTaskView v;
+        v.variant = t.variant;
+        v.settings = t.variant == BC_BC7 ? (const void*)&t.s7 : (const void*)&t.s6;
+        v.src = t.src;
+        v.pitch = t.pitch;
+        v.w = t.w;
+        v.h = t.h;
+        v.dst = t.dst;
+        out.push_back(v);
+    }
+    return BC_OK;
+}
+void compressor_clear(bc_compressor* c) {
+    if (c) c->tasks.clear();
+}
+}  // namespace bcn
+
 // ---- diagnostics ------------------------------------------------------------------------------
 
 extern "C" int bc_last_cuda_error(void) { return t_last_cuda_error; }

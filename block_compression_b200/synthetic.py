@@ -174,3 +174,45 @@ def config4_textures(seed=4, count=64, sides=None):
 
 def config4_texture(seed, index, h, w):
     return rgba8_textured(seed * 1000 + index, w, h, polygons=16)
+
+
+def rgba8_textured_torch(seed, height, width, device, polygons=16):
+    """GPU version of rgba8_textured for large batches: bilinear gradients +
+    4-octave value noise (amplitude 40/255) + filled triangles, alpha 255.
+    Random parameters come from a seeded CPU generator, the pixels are made on
+    `device`. Returns a uint8 tensor (height, width, 4)."""
+    import torch
+    import torch.nn.functional as F
+
+    g = torch.Generator().manual_seed(int(seed))
+    y = torch.linspace(0.0, 1.0, height, device=device)[:, None, None]
+    x = torch.linspace(0.0, 1.0, width, device=device)[None, :, None]
+    c = (torch.rand(2, 2, 3, generator=g) * 255.0).to(device)
+    rgb = c[0, 0] * (1 - y) * (1 - x) + c[0, 1] * (1 - y) * x + c[1, 0] * y * (1 - x) + c[1, 1] * y * x
+    noise = torch.zeros(1, 3, height, width, device=device)
+    amp, total = 1.0, 0.0
+    for o in range(4):
+        cells = 4 * (2 ** o)
+        lat = (torch.rand(1, 3, cells + 1, cells + 1, generator=g) * 2 - 1).to(device)
+        noise += amp * F.interpolate(lat, size=(height, width), mode="bilinear", align_corners=True)
+        total += amp
+        amp *= 0.5
+    rgb = rgb + 40.0 * (noise[0] / total).permute(1, 2, 0)
+    yy = torch.arange(height, device=device, dtype=torch.float32)[:, None] + 0.5
+    xx = torch.arange(width, device=device, dtype=torch.float32)[None, :] + 0.5
+    for _ in range(polygons):
+        cx, cy = float(torch.rand(1, generator=g)) * width, float(torch.rand(1, generator=g)) * height
+        r = (0.03 + 0.22 * float(torch.rand(1, generator=g))) * min(height, width)
+        ang = torch.sort(torch.rand(3, generator=g) * 6.283185307)[0]
+        px = [cx + r * float(torch.cos(a)) for a in ang]
+        py = [cy + r * float(torch.sin(a)) for a in ang]
+        inside = torch.ones(height, width, dtype=torch.bool, device=device)
+        for i in range(3):
+            ax, ay, bx, by = px[i], py[i], px[(i + 1) % 3], py[(i + 1) % 3]
+            inside &= (bx - ax) * (yy - ay) - (by - ay) * (xx - ax) >= 0
+        col = (torch.rand(3, generator=g) * 255.0).to(device)
+        rgb = torch.where(inside[..., None], col, rgb)
+    out = torch.empty(height, width, 4, dtype=torch.uint8, device=device)
+    out[..., :3] = rgb.round().clamp(0, 255).to(torch.uint8)
+    out[..., 3] = 255
+    return out

@@ -193,6 +193,54 @@ int bc_compressor_compress(bc_compressor* c, void* stream);
 /* Number of pending tasks. */
 int bc_compressor_task_count(const bc_compressor* c);
 
+/* ---- batched compression (no counterpart in the reference: the reference
+ * dispatches one compute shader per task, src/block_compressor.rs:550-589) --
+ *
+ * A bc_batch freezes every pending task of a compressor (the compressor's
+ * queue is drained) into one device task table and one CUDA graph: one
+ * persistent work-queue launch for all BC1-BC5 tiles, one pass of the BC7
+ * kernel pipeline over the tiles of all BC7 tasks with the same settings,
+ * one launch per BC6H task. bc_batch_launch replays the graph; the tasks'
+ * buffers must stay valid while the batch exists.
+ *
+ * bc_tune is the launch shape. threads_per_cta: 128 or 256 (BC1-BC5 work
+ * queue); ctas_per_sm: resident CTAs per SM of that queue (1-16);
+ * tiles_per_claim: tiles of 32 blocks a warp takes per queue claim (1-64);
+ * bc7_search_warps: 4 or 8 partition candidates per BC7 search CTA (one
+ * staged tile shared by that many candidate warps). */
+typedef struct bc_tune {
+    uint32_t threads_per_cta;
+    uint32_t ctas_per_sm;
+    uint32_t tiles_per_claim;
+    uint32_t bc7_search_warps;
+} bc_tune;
+
+typedef struct bc_batch bc_batch;
+
+/* tune: explicit launch shape, or NULL. With NULL the shape comes from this
+ * process's autotune cache for a batch of the same shape on the same device;
+ * failing that, autotune != 0 times the candidate shapes on the batch itself
+ * (running it several times on `stream`, writing the outputs) and caches the
+ * winner, and autotune == 0 uses defaults. */
+int bc_batch_create(bc_compressor* c, const bc_tune* tune, int autotune, void* stream, bc_batch** out);
+int bc_batch_launch(bc_batch* b, void* stream);
+int bc_batch_get_tune(const bc_batch* b, bc_tune* out);
+int bc_batch_destroy(bc_batch* b);
+
+/* One-shot: bc_batch_create (autotuned unless `tune` is given),
+ * bc_batch_launch, synchronise `stream`, bc_batch_destroy. */
+int bc_compressor_compress_batched(bc_compressor* c, void* stream, const bc_tune* tune);
+
+/* ---- mip generation (no counterpart in the reference: callers supply mip
+ * levels, src/block_compressor.rs:297-299) ------------------------------------
+ * One mip level of an RGBA8 image: (sw, sh) -> (max(1, sw/2), max(1, sh/2)),
+ * each pixel the 2x2 box average (coordinates clamped to the source,
+ * (sum + 2) / 4 per channel), written padded up to multiples of 4 by edge
+ * replication so the level can be block-compressed directly. dst_pitch >=
+ * padded width * 4 bytes; all pointers and pitches 4-byte aligned. */
+int bc_mip_level_rgba8_device(const uint8_t* src, size_t src_pitch, uint32_t sw, uint32_t sh,
+                              uint8_t* dst, size_t dst_pitch, size_t dst_len, void* stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* cudaError_t of the last CUDA failure seen on this thread (0 if none). */
 int bc_last_cuda_error(void);
