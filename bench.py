@@ -445,6 +445,70 @@ def batched_mips_bench(args):
     batch.close()
 
 
+def refine_bench(args):
+    """Gradient endpoint refinement workload: 8 RGBA8 images of 512x512 (the
+    BC1 generator, seeds 100..107), encoded by the plain BC7 encoder (basic
+    opaque profile) and by BC1, then 20 Adam steps at lr 0.5 per block with
+    keep-if-better. Reports the refinement kernel's time, the PSNR before and
+    after (RGB, exact decoded texels) and the share of blocks replaced, with
+    the oracle's sequential restatement timed on one image beside it. Prints
+    one line (not the benchmark contract line)."""
+    import numpy as np
+    import torch
+
+    import block_compression_b200 as bcn
+    from block_compression_b200 import refine, synthetic
+
+    dev = torch.device("cuda", 0)
+    V = bcn.CompressionVariant
+    imgs = [synthetic.config1_image(100 + i, 512) for i in range(8)]
+    timgs = [torch.from_numpy(im).to(dev) for im in imgs]
+    px = 8 * 512 * 512
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {"workload": "8 RGBA8 images 512x512, 20 Adam steps lr 0.5, keep-if-better", "steps": args.steps}
+    for name, variant, per in (("bc7_opaque_basic", V.BC7(bcn.BC7Settings.opaque_basic()), 16), ("bc1", V.BC1, 8)):
+        orig = []
+        for t in timgs:
+            b = torch.zeros(variant.blocks_byte_size(512, 512), dtype=torch.uint8, device=dev)
+            bcn.encode.compress_rgba8(variant, t, b, 512, 512, 512 * 4)
+            orig.append(b)
+        work = [b.clone() for b in orig]
+        stats = torch.zeros(4, dtype=torch.int64, device=dev)
+        times = []
+        for i in range(args.warmup + args.steps):
+            for w, o in zip(work, orig):
+                w.copy_(o)
+            stats.zero_()
+            torch.cuda.synchronize()
+            a, b = ev(), ev()
+            a.record()
+            for t, w in zip(timgs, work):
+                if per == 16:
+                    refine.refine_bc7(t, w, channels=3, steps=20, lr=0.5, stats=stats)
+                else:
+                    refine.refine_bc1(t, w, steps=20, lr=0.5, stats=stats)
+            b.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                times.append(a.elapsed_time(b))
+        s = stats.cpu().tolist()
+        ms = sum(times) / len(times)
+        psnr = lambda e: 10 * np.log10(255.0 ** 2 / (e / (px * 3)))  # noqa: E731
+        res = {"refine_ms": ms, "refine_mpx_s": px / ms / 1e3, "blocks": s[0], "replaced": s[1],
+               "replaced_frac": s[1] / max(1, s[0]), "psnr_before": psnr(s[2]), "psnr_after": psnr(s[3]),
+               "sq_err_before": s[2], "sq_err_after": s[3]}
+        if not args.no_cpu:
+            import oracle
+            blk = orig[0].cpu().numpy().reshape(-1, per)
+            src = oracle.image_blocks(imgs[0], 512, 512)
+            t0 = time.perf_counter()
+            oracle.refine_blocks("bc7" if per == 16 else "bc1", blk, src, 20, 0.5, 3)
+            dt = time.perf_counter() - t0
+            res["cpu_port"] = {"mpx_s": 512 * 512 / dt / 1e6, "cores": 1, "sample": "1 image 512x512"}
+        out[name] = res
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -453,8 +517,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--case", default=None, help="profiling case VARIANT:SIZE, e.g. bc7:512 (not a bench line)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "mips"],
-                    help="c2: the benchmark line; mips: batched mixed mip-chain workload (extra line)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "mips", "refine"],
+                    help="c2: the benchmark line; mips: batched mixed mip-chain workload; refine: gradient "
+                         "endpoint refinement (extra lines)")
     ap.add_argument("--textures", type=int, default=64)
     args = ap.parse_args()
     world, rank, local = _dist()
@@ -462,6 +527,8 @@ def main():
         profile_case(args)
     elif args.workload == "mips":
         batched_mips_bench(args)
+    elif args.workload == "refine":
+        refine_bench(args)
     elif args.impl == "reference":
         cpu_reference(args, world, rank)
     else:

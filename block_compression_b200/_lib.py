@@ -20,6 +20,7 @@ STATUS_NAMES = {
     -7: "BC_ERR_CUDA",
     -8: "BC_ERR_TASKS",
     -9: "BC_ERR_NO_DEVICE",
+    -10: "BC_ERR_TOO_LARGE",
 }
 
 
@@ -67,6 +68,14 @@ def _load():
         "bc_compressor_compress_batched": ([P, P, P], I),
         "bc_compress_bc7_device_noalloc": ([P, P, S, P, S, U32, U32, S, P], I),
         "bc_mip_level_rgba8_device": ([P, S, U32, U32, P, S, S, P], I),
+        "bc_bc7_parse_device": ([P, S, P, P, P], I),
+        "bc_bc7_decode_relaxed_device": ([P, P, S, P, P], I),
+        "bc_bc7_decode_adjoint_device": ([P, P, S, P, P], I),
+        "bc_bc1_parse_device": ([P, S, P, P, P], I),
+        "bc_bc1_decode_relaxed_device": ([P, P, S, P, P], I),
+        "bc_bc1_decode_adjoint_device": ([P, P, S, P, P], I),
+        "bc_bc7_refine_device": ([P, S, U32, U32, P, S, U32, U32, ctypes.c_float, P, P, P], I),
+        "bc_bc1_refine_device": ([P, S, U32, U32, P, S, U32, ctypes.c_float, P, P, P], I),
         "bc_last_cuda_error": ([], I),
         "bc_version": ([], ctypes.c_char_p),
     }

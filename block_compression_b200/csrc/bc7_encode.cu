@@ -32,387 +32,11 @@
 #include "bc_common.cuh"
 #include "bc_kernels.h"
 #include "bptc_math.cuh"
+#include "bc7_device.cuh"
 namespace bcn {
 namespace bc7 {
 
 using namespace bptc;
-
-// Mode 4/5 candidate block (bc7.rs:680-696): channel `rot` replaced by alpha
-// (4-channel settings) or by 255 (3-channel settings).
-template <bool CH4>
-struct BlkRot {
-    const float* p;
-    int rot;
-    BCN_DEV float operator()(int c, int k) const {
-        if (c == rot) return CH4 ? p[(48 + k) * NB] : 255.0f;
-        return p[(c * 16 + k) * NB];
-    }
-};
-
-// ---- endpoint quantisation (bc7.rs:97-237) ----------------------------------
-
-// ep_quant0367 for one endpoint pair (8 values). QCH = channels quantised
-// (the error uses the first CH); EPB_MODE0 unpacks the trial values to bytes
-// as the reference does for mode 0 only.
-template <int BITS, int CH, int QCH, bool MODE0>
-BCN_DEV void quant0367_pair(int* qep, const float* ep) {
-    constexpr int levels2 = (1 << BITS) * 2 - 1;
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        int qb[2][4];
-        float eb[2][4];
-#pragma unroll
-        for (int b = 0; b < 2; b++) {
-#pragma unroll
-            for (int p = 0; p < QCH; p++) {
-                int v = (int)((ep[i * 4 + p] / 255.0f * (float)levels2 - (float)b) / 2.0f + 0.5f) * 2 + b;
-                qb[b][p] = clampi(v, b, levels2 - 1 + b);
-                eb[b][p] = MODE0 ? (float)unpack_to_byte(qb[b][p], 5) : (float)qb[b][p];
-            }
-        }
-        float err0 = 0.0f, err1 = 0.0f;
-#pragma unroll
-        for (int p = 0; p < CH; p++) {
-            err0 += sqf(ep[i * 4 + p] - eb[0][p]);
-            err1 += sqf(ep[i * 4 + p] - eb[1][p]);
-        }
-#pragma unroll
-        for (int p = 0; p < QCH; p++) qep[i * 4 + p] = err0 < err1 ? qb[0][p] : qb[1][p];
-    }
-}
-
-// ep_quant1 for one pair (shared p-bit)
-BCN_DEV void quant1_pair(int* qep, const float* ep) {
-    int qb[2][8];
-    float eb[2][8];
-#pragma unroll
-    for (int b = 0; b < 2; b++) {
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            if ((i & 3) == 3) continue;  // channel 3 is neither coded nor in the error
-            int v = (int)((ep[i] / 255.0f * 127.0f - (float)b) / 2.0f + 0.5f) * 2 + b;
-            qb[b][i] = clampi(v, b, 126 + b);
-            eb[b][i] = (float)unpack_to_byte(qb[b][i], 7);
-        }
-    }
-    float err0 = 0.0f, err1 = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 2; j++)
-#pragma unroll
-        for (int p = 0; p < 3; p++) {
-            err0 += sqf(ep[j * 4 + p] - eb[0][j * 4 + p]);
-            err1 += sqf(ep[j * 4 + p] - eb[1][j * 4 + p]);
-        }
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if ((i & 3) != 3) qep[i] = err0 < err1 ? qb[0][i] : qb[1][i];
-}
-
-template <int BITS, int N>
-BCN_DEV void quant245(int* qep, const float* ep) {
-    constexpr int levels = 1 << BITS;
-#pragma unroll
-    for (int i = 0; i < N; i++) qep[i] = clampi((int)(ep[i] / 255.0f * (float)(levels - 1) + 0.5f), 0, levels - 1);
-}
-
-// ep_quant_dequant for the partitioned modes over PAIRS pairs; channel 3 is
-// handled only for mode 7 (4 channels).
-template <int MODE>
-BCN_DEV void quant_dequant_part(int qep[24], float ep[24]) {
-    constexpr int pairs = (MODE == 0 || MODE == 2) ? 3 : 2;
-#pragma unroll
-    for (int j = 0; j < pairs; j++) {
-        int* q = qep + 8 * j;
-        float* e = ep + 8 * j;
-        if (MODE == 0) quant0367_pair<4, 3, 3, true>(q, e);
-        else if (MODE == 3) quant0367_pair<7, 3, 3, false>(q, e);
-        else if (MODE == 7) quant0367_pair<5, 4, 4, false>(q, e);
-        else if (MODE == 1) quant1_pair(q, e);
-        else {
-#pragma unroll
-            for (int i = 0; i < 8; i++)
-                if ((i & 3) != 3) q[i] = clampi((int)(e[i] / 255.0f * 31.0f + 0.5f), 0, 31);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            if (MODE != 7 && (i & 3) == 3) continue;
-            if (MODE == 3) e[i] = (float)q[i];
-            else if (MODE == 1) e[i] = (float)unpack_to_byte(q[i], 7);
-            else if (MODE == 7) e[i] = (float)unpack_to_byte(q[i], 6);
-            else e[i] = (float)unpack_to_byte(q[i], 5);
-        }
-    }
-}
-
-// ---- candidate evaluation of modes 0/1/2/3/7 (bc7.rs:517-538) -----------------
-
-template <int MODE>
-struct ModeTraits {
-    static constexpr int bits = (MODE == 0 || MODE == 1) ? 3 : 2;
-    static constexpr int pairs = (MODE == 0 || MODE == 2) ? 3 : 2;
-    static constexpr int ch = MODE == 7 ? 4 : 3;
-};
-
-template <int MODE>
-BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1) {
-    using T = ModeTraits<MODE>;
-    float ep[24];
-#pragma unroll
-    for (int i = 0; i < 24; i++) ep[i] = 0.0f;
-    uint32_t pattern = map[part_id];
-#pragma unroll
-    for (int j = 0; j < T::pairs; j++)
-        block_segment<T::ch, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
-    quant_dequant_part<MODE>(qep, ep);
-    return block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
-}
-
-// bc7.rs:381-440
-template <int MODE>
-BCN_DEV uint4 code_mode01237(int qep[24], uint32_t q0, uint32_t q1, int part_id) {
-    using T = ModeTraits<MODE>;
-    uint32_t flips = apply_swap_mode01237(qep, q0, q1, MODE, part_id);
-    BitWriter bw;
-    bw.clear();
-    bw.put(MODE + 1, 1u << MODE);
-    if (MODE == 0) bw.put(4, (uint32_t)(part_id & 15));
-    else bw.put(6, (uint32_t)(part_id & 63));
-#pragma unroll
-    for (int p = 0; p < T::ch; p++)
-#pragma unroll
-        for (int j = 0; j < T::pairs * 2; j++) {
-            uint32_t v = (uint32_t)qep[j * 4 + p];
-            if (MODE == 0) bw.put(4, v >> 1);
-            else if (MODE == 1) bw.put(6, v >> 1);
-            else if (MODE == 2) bw.put(5, v);
-            else if (MODE == 3) bw.put(7, v >> 1);
-            else bw.put(5, v >> 1);
-        }
-    if (MODE == 1)
-        for (int j = 0; j < 2; j++) bw.put(1, (uint32_t)qep[j * 8] & 1);
-    if (MODE == 0 || MODE == 3 || MODE == 7)
-#pragma unroll
-        for (int j = 0; j < T::pairs * 2; j++) bw.put(1, (uint32_t)qep[j * 4] & 1);
-    code_qblock(bw, q0, q1, T::bits, flips);
-    adjust_skip_mode01237(bw.d, MODE, part_id);
-    return make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
-}
-
-// Refinement of a mode's winning partition (bc7.rs:571-609), then coding.
-template <int MODE>
-BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, float best_err, uint32_t iters,
-                              float opaque_err, uint4& out) {
-    using T = ModeTraits<MODE>;
-    int best_qep[24];
-    uint32_t bq0, bq1;
-    eval_part<MODE>(blk, map, part_id, best_qep, bq0, bq1);  // re-creates the winner's state
-    uint32_t pattern = map[part_id];
-    for (uint32_t it = 0; it < iters; it++) {
-        float ep[24];
-#pragma unroll
-        for (int i = 0; i < 24; i++) ep[i] = 0.0f;
-#pragma unroll
-        for (int j = 0; j < T::pairs; j++)
-            opt_endpoints<T::ch, T::bits>(ep + 8 * j, blk, bq0, bq1, subset_mask_from_map(pattern, j));
-        int qep[24];
-        uint32_t q0, q1;
-        quant_dequant_part<MODE>(qep, ep);
-        float err = block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
-        if (err < best_err) {
-#pragma unroll
-            for (int i = 0; i < 24; i++) best_qep[i] = qep[i];
-            bq0 = q0;
-            bq1 = q1;
-            best_err = err;
-        }
-    }
-    if (MODE != 7) best_err += opaque_err;
-    out = code_mode01237<MODE>(best_qep, bq0, bq1, part_id);
-    return best_err;
-}
-
-// ---- mode 4/5 (bc7.rs:239-369, 442-492, 657-733) ---------------------------------
-
-BCN_DEV void channel_quant_dequant(int qep[2], float ep[2], int epbits) {
-    int elevels = 1 << epbits;
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        qep[i] = clampi((int)(ep[i] / 255.0f * (float)(elevels - 1) + 0.5f), 0, elevels - 1);
-        ep[i] = (float)unpack_to_byte(qep[i], epbits);
-    }
-}
-
-BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const float cb[16], int bits, const float ep[2]) {
-    int levels = 1 << bits;
-    q0 = 0;
-    q1 = 0;
-    float total = 0.0f;
-    int ia = (int)ep[0], ib = (int)ep[1];
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        float proj = (cb[k] - ep[0]) / (ep[1] - ep[0] + 0.001f);
-        int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
-        int w0 = unquant_w(bits, q1i - 1), w1 = unquant_w(bits, q1i);
-        float d0 = (float)(((64 - w0) * ia + w0 * ib + 32) / 64);
-        float d1 = (float)(((64 - w1) * ia + w1 * ib + 32) / 64);
-        float err0 = 0.0f, err1 = 0.0f;
-        err0 += sqf(d0 - cb[k]);
-        err1 += sqf(d1 - cb[k]);
-        float be = err0 < err1 ? err0 : err1;
-        int bq = err0 < err1 ? q1i - 1 : q1i;
-        if (k < 8) q0 |= (uint32_t)bq << (4 * k);
-        else q1 |= (uint32_t)bq << (4 * (k - 8));
-        total += be;
-    }
-    return total;
-}
-
-BCN_DEV void channel_opt_endpoints(float ep[2], const float cb[16], int bits, uint32_t q0, uint32_t q1) {
-    int levels = 1 << bits;
-    float lm1 = (float)(levels - 1);
-    float atb1 = 0.0f, sum_q = 0.0f, sum_qq = 0.0f, sum = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        float q = (float)(((k < 8 ? q0 : q1) >> (4 * (k & 7))) & 15);
-        float x = lm1 - q;
-        sum_q += q;
-        sum_qq += q * q;
-        sum += cb[k];
-        atb1 += x * cb[k];
-    }
-    float atb2 = lm1 * sum - atb1;
-    float cxx = 16.0f * sqf(lm1) - 2.0f * lm1 * sum_q + sum_qq;
-    float cyy = sum_qq;
-    float cxy = lm1 * sum_q - sum_qq;
-    float det = cxx * cyy - cxy * cxy;
-    float scale = lm1 / det;
-    ep[0] = clampf_r((atb1 * cyy - atb2 * cxy) * scale, 0.0f, 255.0f);
-    ep[1] = clampf_r((atb2 * cxx - atb1 * cxy) * scale, 0.0f, 255.0f);
-    if (fabsf(det) < 0.001f) {
-        ep[0] = sum / 16.0f;
-        ep[1] = ep[0];
-    }
-}
-
-// One mode-4/5 candidate: rotation `rot`, index swap SWAP (mode 4 only),
-// CH4 = 4-channel settings. Returns its error and its coded block
-// (bc7_code_mode45 for MODE). The index widths are compile-time so that one
-// launch runs a single instruction stream.
-template <int MODE, int SWAP, bool CH4>
-BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t refine_channel, int rot, uint4& out) {
-    constexpr int bits = SWAP ? 3 : 2;
-    constexpr int abits = SWAP ? 2 : (MODE == 4 ? 3 : 2);
-    constexpr int aepbits = MODE == 4 ? 6 : 8;
-    const int swap = SWAP;
-    BlkRot<CH4> cb{pxlane, rot < 3 ? rot : -1};
-    float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    block_segment<3, true>(cb, 0xFFFFu, ep);
-    int qep[8];
-    constexpr int EPB = MODE == 4 ? 5 : 7;
-    quant245<EPB, 8>(qep, ep);
-#pragma unroll
-    for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
-    uint32_t q0, q1;
-    float err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
-    for (uint32_t it = 0; it < refine; it++) {
-        opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
-        quant245<EPB, 8>(qep, ep);
-#pragma unroll
-        for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
-        err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
-    }
-    // scalar channel (opt_channel, bc7.rs:239-266)
-    float chan[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) chan[k] = pxlane[(rot * 16 + k) * NB];
-    float aep[2] = {255.0f, 0.0f};
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        aep[0] = fminf(aep[0], chan[k]);
-        aep[1] = fmaxf(aep[1], chan[k]);
-    }
-    int aqep[2];
-    uint32_t a0, a1;
-    channel_quant_dequant(aqep, aep, aepbits);
-    float aerr = channel_opt_quant(a0, a1, chan, abits, aep);
-    for (uint32_t it = 0; it < refine_channel; it++) {
-        channel_opt_endpoints(aep, chan, abits, a0, a1);
-        channel_quant_dequant(aqep, aep, aepbits);
-        aerr = channel_opt_quant(a0, a1, chan, abits, aep);
-    }
-    err += aerr;
-
-    // bc7_code_mode45 (bc7.rs:442-492)
-    const int cbits = 2, cabits = MODE == 4 ? 3 : 2, cepbits = MODE == 4 ? 5 : 7, caepbits = MODE == 4 ? 6 : 8;
-    uint32_t c0 = q0, c1 = q1, d0 = a0, d1 = a1;
-    if (swap == 0) {
-        apply_swap_mode456(qep, 4, c0, c1, cbits);
-        apply_swap_mode456(aqep, 1, d0, d1, cabits);
-    } else {
-        uint32_t t0 = c0, t1 = c1;
-        c0 = d0;
-        c1 = d1;
-        d0 = t0;
-        d1 = t1;
-        apply_swap_mode456(aqep, 1, c0, c1, cbits);
-        apply_swap_mode456(qep, 4, d0, d1, cabits);
-    }
-    BitWriter bw;
-    bw.clear();
-    bw.put(MODE + 1, 1u << MODE);
-    bw.put(2, (uint32_t)(rot + 1) & 3);
-    if (MODE == 4) bw.put(1, (uint32_t)swap);
-#pragma unroll
-    for (int p = 0; p < 3; p++) {
-        bw.put(cepbits, (uint32_t)qep[p]);
-        bw.put(cepbits, (uint32_t)qep[4 + p]);
-    }
-    bw.put(caepbits, (uint32_t)aqep[0]);
-    bw.put(caepbits, (uint32_t)aqep[1]);
-    code_qblock(bw, c0, c1, cbits, 0);
-    code_qblock(bw, d0, d1, cabits, 0);
-    out = make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
-    return err;
-}
-
-// ---- mode 6 (bc7.rs:494-515, 762-817) -------------------------------------------
-
-template <int CH>
-BCN_DEV float mode6(const Blk& blk, uint32_t refine, uint4& out) {
-    float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    block_segment<CH, true>(blk, 0xFFFFu, ep);
-    if (CH == 3) {
-        ep[3] = 255.0f;
-        ep[7] = 255.0f;
-    }
-    int qep[8];
-    quant0367_pair<7, CH, 4, false>(qep, ep);
-#pragma unroll
-    for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
-    uint32_t q0, q1;
-    float err = block_quant<CH, 4, 1>(blk, ep, 0, q0, q1);
-    for (uint32_t it = 0; it < refine; it++) {
-        opt_endpoints<CH, 4>(ep, blk, q0, q1, 0xFFFFu);
-        quant0367_pair<7, CH, 4, false>(qep, ep);
-#pragma unroll
-        for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
-        err = block_quant<CH, 4, 1>(blk, ep, 0, q0, q1);
-    }
-    apply_swap_mode456(qep, 4, q0, q1, 4);
-    BitWriter bw;
-    bw.clear();
-    bw.put(7, 64);
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-        bw.put(7, (uint32_t)qep[p] >> 1);
-        bw.put(7, (uint32_t)qep[4 + p] >> 1);
-    }
-    bw.put(1, (uint32_t)qep[0] & 1);
-    bw.put(1, (uint32_t)qep[4] & 1);
-    code_qblock(bw, q0, q1, 4, 0);
-    out = make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
-    return err;
-}
 
 // ---- kernels --------------------------------------------------------------------
 

@@ -241,6 +241,62 @@ int bc_compressor_compress_batched(bc_compressor* c, void* stream, const bc_tune
 int bc_mip_level_rgba8_device(const uint8_t* src, size_t src_pitch, uint32_t sw, uint32_t sh,
                               uint8_t* dst, size_t dst_pitch, size_t dst_len, void* stream);
 
+/* ---- differentiable decode and gradient endpoint refinement (no counterpart
+ * in the reference) -------------------------------------------------------------
+ * The relaxed decode replaces a block's quantised endpoints by continuous
+ * endpoints in 8-bit units and drops the decoder's integer rounding, for a
+ * fixed mode, partition, rotation, index selector and fixed indices:
+ *   BC7: c = e0 + (e1 - e0) * w / 64, w the BPTC index weight
+ *        (src/encode/common.rs:6-21), channels swapped by the block's rotation
+ *        (src/decode/block.rs:1238-1243); modes 0-3 give alpha 255;
+ *   BC1: c = e0 + (e1 - e0) * t, t = 0, 1, 1/3, 2/3 for indices 0..3 in the
+ *        four-colour mode (block.rs:153-165), t = 0, 1, 1/2 and constant
+ *        transparent black for index 3 in the three-colour mode (:166-175).
+ * With the endpoints a parse returns, floor(c + 0.5) equals the decoder's
+ * output. All buffers are device memory; calls are stream-ordered.
+ *
+ * Layouts per block:
+ *   BC7 meta: 8 x uint32 (16-byte aligned), endpoints: 24 x float (slot
+ *       (2 * subset + end) * 4 + channel, RGBA before the rotation swap,
+ *       16-byte aligned);
+ *   BC1 meta: 2 x uint32, endpoints: 6 x float (e0 RGB, e1 RGB);
+ *   relaxed pixels and their gradients: 16 x 4 floats (pixel y * 4 + x,
+ *       RGBA), 16-byte aligned.
+ * A BC7 block with the reserved mode encoding decodes to zeros and has a zero
+ * gradient. */
+int bc_bc7_parse_device(const uint8_t* blocks, size_t nblocks, uint32_t* meta, float* endpoints,
+                        void* stream);
+int bc_bc7_decode_relaxed_device(const uint32_t* meta, const float* endpoints, size_t nblocks,
+                                 float* out, void* stream);
+/* Adjoint of the relaxed decode: grad_endpoints = (d out / d endpoints)^T grad_out. */
+int bc_bc7_decode_adjoint_device(const uint32_t* meta, const float* grad_out, size_t nblocks,
+                                 float* grad_endpoints, void* stream);
+int bc_bc1_parse_device(const uint8_t* blocks, size_t nblocks, uint32_t* meta, float* endpoints,
+                        void* stream);
+int bc_bc1_decode_relaxed_device(const uint32_t* meta, const float* endpoints, size_t nblocks,
+                                 float* out, void* stream);
+int bc_bc1_decode_adjoint_device(const uint32_t* meta, const float* grad_out, size_t nblocks,
+                                 float* grad_endpoints, void* stream);
+
+/* Gradient endpoint refinement of encoded blocks against their RGBA8 source
+ * (width x height, multiples of 4; src_stride in bytes). Per block: `steps`
+ * Adam steps (beta1 0.9, beta2 0.999, eps 1e-8, learning rate `lr` in 8-bit
+ * units) on the relaxed decode's squared error over the first `channels`
+ * channels (BC1: RGB), each step followed by re-quantisation with the
+ * encoder's quantisers and coding with the block's fixed indices
+ * (src/encode/bc7.rs:97-276 and :381-515; src/encode/bc1_to_5.rs:268-278).
+ * The best coded block replaces the input, in place, only if its exact
+ * squared error (decoded texels against the source) is strictly lower.
+ * stats (optional, 4 x uint64, added to, not cleared): blocks refined,
+ * blocks replaced, summed exact error before, after.
+ * endpoints_out (optional): the final continuous endpoints per block. */
+int bc_bc7_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, uint32_t height,
+                         uint8_t* blocks, size_t blocks_len, uint32_t channels, uint32_t steps,
+                         float lr, uint64_t* stats, float* endpoints_out, void* stream);
+int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, uint32_t height,
+                         uint8_t* blocks, size_t blocks_len, uint32_t steps, float lr,
+                         uint64_t* stats, float* endpoints_out, void* stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* cudaError_t of the last CUDA failure seen on this thread (0 if none). */
 int bc_last_cuda_error(void);

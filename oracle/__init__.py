@@ -71,6 +71,17 @@ def lib():
         L.oracle_f16_to_f32.restype = ctypes.c_float
         L.oracle_linear_to_srgb.argtypes = [ctypes.c_float]
         L.oracle_linear_to_srgb.restype = ctypes.c_uint8
+        for name in ("oracle_bc7_parse", "oracle_bc1_parse"):
+            getattr(L, name).argtypes = [P, S, P, P]
+            getattr(L, name).restype = None
+        for name in ("oracle_bc7_relaxed_f64", "oracle_bc7_adjoint_f64", "oracle_bc1_relaxed_f64",
+                     "oracle_bc1_adjoint_f64"):
+            getattr(L, name).argtypes = [P, P, S, P]
+            getattr(L, name).restype = None
+        L.oracle_bc7_refine_block.argtypes = [P, P, U32, U32, ctypes.c_float, P, P]
+        L.oracle_bc7_refine_block.restype = None
+        L.oracle_bc1_refine_block.argtypes = [P, P, U32, ctypes.c_float, P, P]
+        L.oracle_bc1_refine_block.restype = None
         _lib = L
     return _lib
 
@@ -216,3 +227,68 @@ def count_ops(kind, block, settings=None):
         return getattr(L, "oracle_count_" + kind)(_ptr(b))
     keep, sp = _settings_ptr(settings)
     return getattr(L, "oracle_count_" + kind)(_ptr(b), sp)
+
+
+# ---- relaxed (differentiable) decode and endpoint refinement ----------------------
+# Layouts: BC7 meta (n, 8) uint32 + endpoints (n, 24); BC1 meta (n, 2) +
+# endpoints (n, 6); relaxed pixels and gradients (n, 16, 4).
+
+_META_WORDS = {"bc7": 8, "bc1": 2}
+_EP_COUNT = {"bc7": 24, "bc1": 6}
+_BLOCK = {"bc7": 16, "bc1": 8}
+
+
+def parse(kind, blocks):
+    """Parses n blocks (uint8, n * 8 or n * 16 bytes) -> (meta uint32, endpoints float32)."""
+    b = np.ascontiguousarray(blocks, dtype=np.uint8).reshape(-1)
+    n = b.size // _BLOCK[kind]
+    meta = np.zeros((n, _META_WORDS[kind]), dtype=np.uint32)
+    ep = np.zeros((n, _EP_COUNT[kind]), dtype=np.float32)
+    getattr(lib(), "oracle_%s_parse" % kind)(_ptr(b), n, _ptr(meta), _ptr(ep))
+    return meta, ep
+
+
+def relaxed_f64(kind, meta, endpoints):
+    """FP64 relaxed decode -> (n, 16, 4) float64."""
+    meta = np.ascontiguousarray(meta, dtype=np.uint32)
+    ep = np.ascontiguousarray(endpoints, dtype=np.float64)
+    n = meta.shape[0]
+    out = np.zeros((n, 16, 4), dtype=np.float64)
+    getattr(lib(), "oracle_%s_relaxed_f64" % kind)(_ptr(meta), _ptr(ep), n, _ptr(out))
+    return out
+
+
+def adjoint_f64(kind, meta, grad):
+    """FP64 adjoint of the relaxed decode -> (n, endpoints) float64."""
+    meta = np.ascontiguousarray(meta, dtype=np.uint32)
+    g = np.ascontiguousarray(grad, dtype=np.float64)
+    n = meta.shape[0]
+    out = np.zeros((n, _EP_COUNT[kind]), dtype=np.float64)
+    getattr(lib(), "oracle_%s_adjoint_f64" % kind)(_ptr(meta), _ptr(g), n, _ptr(out))
+    return out
+
+
+def refine_blocks(kind, blocks, src_blocks, steps, lr, channels=4):
+    """Sequential restatement of the refinement kernels, block by block.
+    blocks: (n, 8|16) uint8 (copied); src_blocks: (n, 16, 4) uint8 source
+    pixels per block. Returns (refined blocks, final endpoints, errors (n, 2))."""
+    L = lib()
+    out = np.array(blocks, dtype=np.uint8).reshape(-1, _BLOCK[kind]).copy()
+    src = np.ascontiguousarray(src_blocks, dtype=np.uint8).reshape(-1, 64)
+    n = out.shape[0]
+    theta = np.zeros((n, _EP_COUNT[kind]), dtype=np.float32)
+    errs = np.zeros((n, 2), dtype=np.uint32)
+    for i in range(n):
+        bi = out[i]
+        if kind == "bc7":
+            L.oracle_bc7_refine_block(_ptr(bi), _ptr(src[i]), channels, steps, lr, _ptr(theta[i]), _ptr(errs[i]))
+        else:
+            L.oracle_bc1_refine_block(_ptr(bi), _ptr(src[i]), steps, lr, _ptr(theta[i]), _ptr(errs[i]))
+    return out, theta, errs
+
+
+def image_blocks(rgba, width, height):
+    """(h, w, 4) uint8 image -> (n, 16, 4) source pixels, blocks row-major."""
+    img = np.asarray(rgba, dtype=np.uint8).reshape(height, width, 4)
+    t = img.reshape(height // 4, 4, width // 4, 4, 4).transpose(0, 2, 1, 3, 4)
+    return np.ascontiguousarray(t.reshape(-1, 16, 4))

@@ -243,3 +243,94 @@ void bc3_alpha(const real block[64], uint32_t data[2]) {
 }
 
 }  // namespace oracle
+
+#ifndef ORACLE_COUNT_OPS
+// ---- gradient endpoint refinement (no reference counterpart) -------------------
+//
+// BC1 counterpart of oracle_bc7_refine_block: Adam on the relaxed decode's RGB
+// MSE, re-quantisation with enc_rgb565 (bc1_to_5.rs:268-278) and the block's
+// fixed indices. A four-colour block whose endpoints come out in the wrong
+// order is swapped with indices 0<->1, 2<->3 (as the encoder orders them,
+// bc1_to_5.rs:406-409); equal endpoints would decode in the three-colour mode,
+// so every index then points at endpoint 0. A three-colour block keeps
+// colour0 <= colour1 (indices 0<->1 swapped). Kept only on a strictly lower
+// exact RGB error.
+#include "oracle_decode.h"
+#include "oracle_relaxed.h"
+
+namespace oracle {
+static void bc1_requant_code(const uint32_t meta[2], const float theta[6], uint32_t out[2]) {
+    real c0[3], c1[3];
+    for (int c = 0; c < 3; c++) {
+        c0[c] = clampf_r(theta[c], 0.0f, 255.0f);
+        c1[c] = clampf_r(theta[3 + c], 0.0f, 255.0f);
+    }
+    int32_t p0 = enc_rgb565(c0), p1 = enc_rgb565(c1);
+    uint32_t idx = meta[1];
+    bool four = (meta[0] & 0xFFFF) > (meta[0] >> 16);
+    if (four) {
+        if (p0 < p1) {
+            int32_t t = p0;
+            p0 = p1;
+            p1 = t;
+            idx ^= 0x55555555u;
+        } else if (p0 == p1) {
+            idx = 0;
+        }
+    } else if (p0 > p1) {
+        int32_t t = p0;
+        p0 = p1;
+        p1 = t;
+        idx ^= ~(idx >> 1) & 0x55555555u;
+    }
+    out[0] = (uint32_t)p0 | (uint32_t)p1 << 16;
+    out[1] = idx;
+}
+
+static uint32_t bc1_exact_err(const uint32_t words[2], const uint8_t src[64]) {
+    uint8_t bytes[8], px[64];
+    std::memcpy(bytes, words, 8);
+    decode_block_bc1(bytes, px, 16);
+    uint32_t err = 0;
+    for (int k = 0; k < 16; k++)
+        for (int c = 0; c < 3; c++) {
+            int d = (int)px[k * 4 + c] - (int)src[k * 4 + c];
+            err += (uint32_t)(d * d);
+        }
+    return err;
+}
+}  // namespace oracle
+
+extern "C" void oracle_bc1_refine_block(uint8_t blk[8], const uint8_t src[64], uint32_t steps, float lr,
+                                        float* theta_out, uint32_t errs[2]) {
+    using namespace oracle;
+    uint32_t meta[2], best[2];
+    float theta[6], m[6] = {0}, v[6] = {0};
+    relaxed::bc1_parse(blk, meta, theta);
+    std::memcpy(best, blk, 8);
+    uint32_t best_err = bc1_exact_err(best, src);
+    errs[0] = best_err;
+    float s[64], x[64], g[64], ge[6];
+    for (int i = 0; i < 64; i++) s[i] = (float)src[i];
+    float b1t = 1.0f, b2t = 1.0f;
+    for (uint32_t it = 0; it < steps; it++) {
+        relaxed::bc1_relaxed<float>(meta, theta, x);
+        for (int k = 0; k < 16; k++)
+            for (int c = 0; c < 4; c++) g[k * 4 + c] = c < 3 ? 2.0f * (x[k * 4 + c] - s[k * 4 + c]) : 0.0f;
+        relaxed::bc1_adjoint<float>(meta, g, ge);
+        b1t *= 0.9f;
+        b2t *= 0.999f;
+        relaxed::adam_step(theta, m, v, ge, 6, lr, b1t, b2t);
+        uint32_t cand[2];
+        bc1_requant_code(meta, theta, cand);
+        uint32_t err = bc1_exact_err(cand, src);
+        if (err < best_err) {
+            best_err = err;
+            std::memcpy(best, cand, 8);
+        }
+    }
+    std::memcpy(blk, best, 8);
+    errs[1] = best_err;
+    if (theta_out) std::memcpy(theta_out, theta, sizeof(theta));
+}
+#endif

@@ -540,3 +540,107 @@ void bc7_encode_block(const real block[64], const BC7Settings* settings, uint32_
 }
 
 }  // namespace oracle
+
+#ifndef ORACLE_COUNT_OPS
+// ---- gradient endpoint refinement (no reference counterpart) -------------------
+//
+// Restatement, for the parity tests, of the BC7 refinement the CUDA kernels
+// run: Adam on the relaxed decode's MSE (oracle_relaxed.h), then after every
+// step the endpoints are re-quantised with the encoder's own ep_quant /
+// channel_quant_dequant (bc7.rs:97-276) and coded with the block's fixed mode,
+// partition, rotation, index selector and indices through bc7_code_*
+// (bc7.rs:381-515, anchor swaps included). A coded block replaces the best so
+// far only if its exact squared error (decoded bytes against the source) is
+// strictly lower.
+#include "oracle_relaxed.h"
+
+namespace oracle {
+namespace {
+
+void bc7_requant_code(const uint32_t meta[8], const float theta[24], uint32_t channels, uint32_t out[4]) {
+    uint32_t mode = meta[0] & 15, partition = (meta[0] >> 4) & 63, rotation = (meta[0] >> 10) & 3;
+    uint32_t isb = (meta[0] >> 12) & 1, subsets = (meta[0] >> 13) & 3;
+    real ep[24];
+    for (int i = 0; i < 24; i++) ep[i] = clampf_r(theta[i], 0.0f, 255.0f);
+    BC7 s;
+    std::memset(s.data, 0, sizeof(s.data));
+    uint32_t qblock[2] = {meta[1], meta[2]};
+    if (mode == 4 || mode == 5) {
+        Mode45Parameters p;
+        ep_quant245(p.qep, ep, mode);
+        real aep[2] = {ep[3], ep[7]};
+        channel_quant_dequant(p.aqep, aep, mode == 4 ? 6 : 8);
+        p.qblock[0] = meta[1];
+        p.qblock[1] = meta[2];
+        p.aqblock[0] = meta[3];
+        p.aqblock[1] = meta[4];
+        p.rotation = (rotation + 3) & 3;  // the stored field is the encoder's rotation + 1
+        p.swap = isb;
+        bc7_code_mode45(s, p, mode);
+    } else if (mode == 6) {
+        int32_t qep[8] = {0};
+        ep_quant(qep, ep, 6, channels);
+        bc7_code_mode6(s, qep, qblock);
+    } else {
+        int32_t qep[24] = {0};
+        ep_quant(qep, ep, mode, mode == 7 ? 4 : 3);
+        int32_t part_id = (int32_t)(subsets == 3 ? 64 + partition : partition);
+        bc7_code_mode01237(s, qep, qblock, part_id, mode);
+    }
+    for (int i = 0; i < 4; i++) out[i] = s.data[i];
+}
+
+uint32_t bc7_exact_err(const uint32_t words[4], const uint8_t src[64], uint32_t channels) {
+    uint8_t bytes[16], px[64];
+    std::memcpy(bytes, words, 16);
+    decode_block_bc7(bytes, px, 16);
+    uint32_t err = 0;
+    for (int k = 0; k < 16; k++)
+        for (uint32_t c = 0; c < channels; c++) {
+            int d = (int)px[k * 4 + c] - (int)src[k * 4 + c];
+            err += (uint32_t)(d * d);
+        }
+    return err;
+}
+
+}  // namespace
+}  // namespace oracle
+
+// blk: 16 bytes, refined in place. src: the block's 16 RGBA8 source pixels
+// (row-major). channels: 3 (RGB error) or 4 (RGBA). theta_out: the final
+// continuous endpoints (may be NULL). errs: {error before, error after}.
+extern "C" void oracle_bc7_refine_block(uint8_t blk[16], const uint8_t src[64], uint32_t channels, uint32_t steps,
+                                        float lr, float* theta_out, uint32_t errs[2]) {
+    using namespace oracle;
+    uint32_t meta[8], best[4];
+    float theta[24], m[24] = {0}, v[24] = {0};
+    relaxed::bc7_parse(blk, meta, theta);
+    std::memcpy(best, blk, 16);
+    uint32_t best_err = bc7_exact_err(best, src, channels);
+    errs[0] = best_err;
+    if ((meta[0] & 15) < 8) {
+        float s[64], x[64], g[64], ge[24];
+        for (int i = 0; i < 64; i++) s[i] = (float)src[i];
+        float b1t = 1.0f, b2t = 1.0f;
+        for (uint32_t it = 0; it < steps; it++) {
+            relaxed::bc7_relaxed<float>(meta, theta, x);
+            for (int k = 0; k < 16; k++)
+                for (uint32_t c = 0; c < 4; c++) g[k * 4 + c] = c < channels ? 2.0f * (x[k * 4 + c] - s[k * 4 + c]) : 0.0f;
+            relaxed::bc7_adjoint<float>(meta, g, ge);
+            b1t *= 0.9f;
+            b2t *= 0.999f;
+            relaxed::adam_step(theta, m, v, ge, 24, lr, b1t, b2t);
+            uint32_t cand[4];
+            bc7_requant_code(meta, theta, channels, cand);
+            uint32_t err = bc7_exact_err(cand, src, channels);
+            if (err < best_err) {
+                best_err = err;
+                std::memcpy(best, cand, 16);
+            }
+        }
+    }
+    std::memcpy(blk, best, 16);
+    errs[1] = best_err;
+    if (theta_out) std::memcpy(theta_out, theta, sizeof(theta));
+}
+#endif
