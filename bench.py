@@ -509,6 +509,60 @@ def refine_bench(args):
     print(json.dumps(out), flush=True)
 
 
+def decode_bench(args):
+    """Decode bandwidth: each variant's blocks of an NxN image (encoded once by
+    the GPU encoders) decoded to RGBA8 (BC6H also to RGBA16F), L2 flushed
+    before every timed launch. Algorithmic bytes per launch = block bytes read
+    + texel bytes written. Prints one line (not the benchmark contract line)."""
+    import torch
+
+    import block_compression_b200 as bcn
+    from block_compression_b200 import synthetic
+
+    dev = torch.device("cuda", 0)
+    V = bcn.CompressionVariant
+    size = args.decode_size
+    peaks, src_kind = _peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    img = synthetic.rgba8_textured_torch(9, size, size, dev)
+    reps = max(1, size // 1024)
+    hdr = torch.from_numpy(synthetic.config3_hdr(seed=3, size=min(size, 1024)).view("int16")).to(dev)
+    hdr = hdr.repeat(reps, reps, 1).contiguous()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {"workload": "decode of %dx%d images, L2 flushed per launch" % (size, size), "hbm_peak_gbs": hbm,
+           "peak_source": src_kind}
+    b6 = V.BC6H(bcn.BC6HSettings.very_fast())
+    cases = [("bc1", V.BC1, 0), ("bc2", V.BC2, 0), ("bc3", V.BC3, 0), ("bc4", V.BC4, 0), ("bc5", V.BC5, 0),
+             ("bc7", V.BC7(bcn.BC7Settings.opaque_ultra_fast()), 0), ("bc6h_rgba8", b6, 0), ("bc6h_rgba16f", b6, 1)]
+    for name, v, fmt in cases:
+        blocks = torch.zeros(v.blocks_byte_size(size, size), dtype=torch.uint8, device=dev)
+        if name.startswith("bc6h"):
+            bcn.encode.compress_rgba16(v, hdr, blocks, size, size, size * 4)
+        else:
+            bcn.encode.compress_rgba8(v, img, blocks, size, size, size * 4)
+        dst = torch.empty(size * size * 4, dtype=torch.int16 if fmt else torch.uint8, device=dev)
+        dec = bcn.decode.decompress_blocks_as_rgba16f if fmt else bcn.decode.decompress_blocks_as_rgba8
+        times = []
+        for i in range(args.warmup + args.steps):
+            flush.fill_(1)
+            a, b = ev(), ev()
+            a.record()
+            dec(v, size, size, blocks, dst)
+            b.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                times.append(a.elapsed_time(b))
+        ms = sum(times) / len(times)
+        # BC6H to RGBA16F writes the RGB triplets only (the reference's layout)
+        written = dst.numel() * dst.element_size() * (3 / 4 if fmt else 1)
+        nbytes = blocks.numel() + written
+        gbs = nbytes / ms / 1e6
+        out[name] = {"ms": ms, "gb_s": gbs, "frac_hbm": gbs / hbm, "bytes_per_launch": int(nbytes),
+                     "mpx_s": size * size / ms / 1e3}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -517,10 +571,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--case", default=None, help="profiling case VARIANT:SIZE, e.g. bc7:512 (not a bench line)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "mips", "refine"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "mips", "refine", "decode"],
                     help="c2: the benchmark line; mips: batched mixed mip-chain workload; refine: gradient "
-                         "endpoint refinement (extra lines)")
+                         "endpoint refinement; decode: decode bandwidth (extra lines)")
     ap.add_argument("--textures", type=int, default=64)
+    ap.add_argument("--decode-size", type=int, default=8192)
     args = ap.parse_args()
     world, rank, local = _dist()
     if args.case:
@@ -529,6 +584,8 @@ def main():
         batched_mips_bench(args)
     elif args.workload == "refine":
         refine_bench(args)
+    elif args.workload == "decode":
+        decode_bench(args)
     elif args.impl == "reference":
         cpu_reference(args, world, rank)
     else:

@@ -39,7 +39,7 @@ class BcError(RuntimeError):
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            "libbcn_b200.so is not built; run `python -m block_compression_b200.build` "
+            "libbcn_b200.so is not built; run `python block_compression_b200/build.py` "
             "(nvcc with sm_100a support is required)")
     L = ctypes.CDLL(LIB_PATH)
     P, S, U32, I = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint32, ctypes.c_int

@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(kThreads) bc1_adjoint_kernel(const uint32_t* _
 
 // ---- fused refinement -----------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads) bc7_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
+__global__ void __launch_bounds__(kThreads) bc7_endpoint_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
                                                               bool src_aligned, uint32_t bw, uint32_t bh,
                                                               uint8_t* __restrict__ blocks, bool blk_aligned,
                                                               uint32_t channels, uint32_t steps, float lr,
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) bc7_refine_kernel(const uint8_t* __r
     add_stats(stats, active, improved, before, after);
 }
 
-__global__ void __launch_bounds__(kThreads) bc1_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
+__global__ void __launch_bounds__(kThreads) bc1_endpoint_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
                                                               bool src_aligned, uint32_t bw, uint32_t bh,
                                                               uint8_t* __restrict__ blocks, bool blk_aligned,
                                                               uint32_t steps, float lr,
@@ -569,7 +569,7 @@ extern "C" int bc_bc7_refine_device(const uint8_t* src, size_t src_stride, uint3
     uint32_t bw = width / 4, bh = height / 4;
     if ((uint64_t)bw * bh == 0) return BC_OK;
     bool src_al = aligned_to(src, 16) && src_stride % 16 == 0;
-    bc7_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
+    bc7_endpoint_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
         src, src_stride, src_al, bw, bh, blocks, aligned_to(blocks, 16), channels, steps, lr,
         reinterpret_cast<unsigned long long*>(stats), endpoints_out);
     return finish_launch();
@@ -583,7 +583,7 @@ extern "C" int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint3
     uint32_t bw = width / 4, bh = height / 4;
     if ((uint64_t)bw * bh == 0) return BC_OK;
     bool src_al = aligned_to(src, 16) && src_stride % 16 == 0;
-    bc1_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
+    bc1_endpoint_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
         src, src_stride, src_al, bw, bh, blocks, aligned_to(blocks, 8), steps, lr,
         reinterpret_cast<unsigned long long*>(stats), endpoints_out);
     return finish_launch();
