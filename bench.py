@@ -41,8 +41,8 @@ W = H = 2048
 OPS_PER_BLOCK = {"bc7_alpha_basic": 354530.4, "bc3": 1155.0, "bc4": 101.4, "bc5": 202.3}
 SMS, FP32_LANES_PER_SM = 148, 128
 # DRAM bytes (read + write) of one BC7 encode of this workload, summed over
-# the pipeline's launches, from an ncu capture (profiles/bc7_pipeline_2048.md).
-BC7_DRAM_BYTES_PER_LAUNCH = None
+# the pipeline's launches, from an ncu capture with warm L2 (--cache-control none).
+BC7_DRAM_BYTES_PER_LAUNCH = 122.8e6
 METRIC ="BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
 WORKLOAD = "2048x2048 RGBA8 alpha texture: BC7 alpha_basic + BC3 + BC4(R); 2048x2048 normal map: BC5"
 
