@@ -534,7 +534,9 @@ def decode_bench(args):
            "peak_source": src_kind}
     b6 = V.BC6H(bcn.BC6HSettings.very_fast())
     cases = [("bc1", V.BC1, 0), ("bc2", V.BC2, 0), ("bc3", V.BC3, 0), ("bc4", V.BC4, 0), ("bc5", V.BC5, 0),
-             ("bc7", V.BC7(bcn.BC7Settings.opaque_ultra_fast()), 0), ("bc6h_rgba8", b6, 0), ("bc6h_rgba16f", b6, 1)]
+             ("bc7_mode6", V.BC7(bcn.BC7Settings.opaque_ultra_fast()), 0),
+             ("bc7_mixed_modes", V.BC7(bcn.BC7Settings.alpha_basic()), 0), ("bc6h_rgba8", b6, 0),
+             ("bc6h_rgba16f", b6, 1)]
     for name, v, fmt in cases:
         blocks = torch.zeros(v.blocks_byte_size(size, size), dtype=torch.uint8, device=dev)
         if name.startswith("bc6h"):

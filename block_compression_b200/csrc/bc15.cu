@@ -306,28 +306,26 @@ __global__ void __launch_bounds__(128) bc15_encode_kernel(const uint8_t* __restr
 
 // ---- BC1-BC5 decode (src/decode/block.rs:124-258, src/decode.rs:60-148) ------
 
-BCN_DEV void decode_smooth(uint32_t lo, uint32_t hi, uint8_t out[16]) {
-    uint32_t a[8];
-    a[0] = lo & 0xFF;
-    a[1] = (lo >> 8) & 0xFF;
-    if (a[0] > a[1]) {
-        a[2] = (6 * a[0] + a[1]) / 7;
-        a[3] = (5 * a[0] + 2 * a[1]) / 7;
-        a[4] = (4 * a[0] + 3 * a[1]) / 7;
-        a[5] = (3 * a[0] + 4 * a[1]) / 7;
-        a[6] = (2 * a[0] + 5 * a[1]) / 7;
-        a[7] = (a[0] + 6 * a[1]) / 7;
+// block.rs:221-258. The 8-entry palette is kept as 8 bytes in two registers
+// and indexed with a byte permute (no local-memory array).
+BCN_DEV void decode_smooth(uint32_t lo, uint32_t hi, uint32_t out[16]) {
+    uint32_t a0 = lo & 0xFF, a1 = (lo >> 8) & 0xFF;
+    uint32_t p_lo, p_hi;
+    if (a0 > a1) {
+        p_lo = a0 | (a1 << 8) | (((6 * a0 + a1) / 7) << 16) | (((5 * a0 + 2 * a1) / 7) << 24);
+        p_hi = ((4 * a0 + 3 * a1) / 7) | (((3 * a0 + 4 * a1) / 7) << 8) | (((2 * a0 + 5 * a1) / 7) << 16) |
+               (((a0 + 6 * a1) / 7) << 24);
     } else {
-        a[2] = (4 * a[0] + a[1]) / 5;
-        a[3] = (3 * a[0] + 2 * a[1]) / 5;
-        a[4] = (2 * a[0] + 3 * a[1]) / 5;
-        a[5] = (a[0] + 4 * a[1]) / 5;
-        a[6] = 0;
-        a[7] = 255;
+        p_lo = a0 | (a1 << 8) | (((4 * a0 + a1) / 5) << 16) | (((3 * a0 + 2 * a1) / 5) << 24);
+        p_hi = ((2 * a0 + 3 * a1) / 5) | (((a0 + 4 * a1) / 5) << 8) | (0u << 16) | (255u << 24);
     }
-    uint64_t idx = ((uint64_t)hi << 16) | (lo >> 16);
+    // 48 index bits: pixels 0-7 in the low 24, pixels 8-15 in the high 24
+    uint32_t i0 = (lo >> 16) | ((hi & 0xFF) << 16), i1 = hi >> 8;
 #pragma unroll
-    for (int k = 0; k < 16; k++) out[k] = (uint8_t)a[(idx >> (3 * k)) & 7];
+    for (int k = 0; k < 16; k++) {
+        uint32_t sel = ((k < 8 ? i0 : i1) >> (3 * (k & 7))) & 7u;
+        out[k] = __byte_perm(p_lo, p_hi, sel) & 0xFFu;
+    }
 }
 
 // Decodes one BC1-BC5 block to 16 RGBA8 pixels, with the reference's RGBA8
@@ -344,21 +342,18 @@ BCN_DEV void decode_bc15_rgba8(int variant, const uint32_t* w, uint32_t out[16])
         }
     } else if (variant == BC_BC3) {
         decode_color(w[2], w[3], true, out);
-        uint8_t a[16];
+        uint32_t a[16];
         decode_smooth(w[0], w[1], a);
 #pragma unroll
-        for (int k = 0; k < 16; k++) out[k] = (out[k] & 0x00FFFFFFu) | ((uint32_t)a[k] << 24);
+        for (int k = 0; k < 16; k++) out[k] = (out[k] & 0x00FFFFFFu) | (a[k] << 24);
     } else if (variant == BC_BC4) {
-        uint8_t r[16];
-        decode_smooth(w[0], w[1], r);
-#pragma unroll
-        for (int k = 0; k < 16; k++) out[k] = r[k];
+        decode_smooth(w[0], w[1], out);
     } else {
-        uint8_t r[16], g[16];
+        uint32_t r[16], g[16];
         decode_smooth(w[0], w[1], r);
         decode_smooth(w[2], w[3], g);
 #pragma unroll
-        for (int k = 0; k < 16; k++) out[k] = (uint32_t)r[k] | ((uint32_t)g[k] << 8);
+        for (int k = 0; k < 16; k++) out[k] = r[k] | (g[k] << 8);
     }
 }
 

@@ -214,14 +214,26 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
         g[i] = unquantize_u(g[i], bits0);
         b[i] = unquantize_u(b[i], bits0);
     }
-    int ib = mode >= 10 ? 4 : 3;
+    // Index bits: 46 bits from bit 82 (two subsets, 3-bit indices) or 63 bits
+    // from bit 65 (one subset, 4-bit); a zero is re-inserted above each anchor
+    // index so that pixel k's index sits at bits [k*ib, k*ib + ib).
+    const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
+    uint32_t map = 0;
+    uint64_t x;
+    if (mode >= 10) {
+        x = insert_zero(bits64_at(d, 65), 3);
+    } else {
+        x = insert_zero(bits64_at(d, 82) & ((1ull << 46) - 1ull), 2);
+        uint32_t a1 = __ldg(&kDecAnchors[part]) >> 4;
+        x = insert_zero(x, a1 * 3 + 2);
+        map = __ldg(&kDecPartitionMap[part]);
+    }
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        uint32_t ps = mode >= 10 ? (k == 0 ? 0x80u : 0u) : partition_set((uint32_t)part, k);
-        int nb = (ps & 0x80) ? ib - 1 : ib;
-        int idx = bs.ri(nb);
-        int e = (ps & 1) ? 2 : 0;
-        int w = w_of(ib, idx);
+        int w;
+        if (mode >= 10) w = (int)bptc_weight<4>((uint32_t)(x >> (4 * k)) & 15u);
+        else w = (int)bptc_weight<3>((uint32_t)(x >> (3 * k)) & 7u);
+        bool e = ((map >> (2 * k)) & 1u) != 0;
         int r0 = e ? r[2] : r[0], r1 = e ? r[3] : r[1];
         int g0 = e ? g[2] : g[0], g1 = e ? g[3] : g[1];
         int b0 = e ? b[2] : b[0], b1 = e ? b[3] : b[1];
@@ -237,30 +249,66 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
 __device__ uint8_t g_half_to_srgb[0x7C00];
 
 __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
-                                                          void* __restrict__ out, size_t pitch, int fmt) {
+                                                          void* __restrict__ out, size_t pitch, int fmt, bool aligned) {
     uint32_t n = bw * bh;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t by = i / bw, bx = i - by * bw;
         const uint8_t* b = blocks + (size_t)i * 16;
         uint64_t lo = 0, hi = 0;
-        for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
-        for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        if (aligned) {
+            uint4 v = __ldg(reinterpret_cast<const uint4*>(b));
+            lo = (uint64_t)v.x | ((uint64_t)v.y << 32);
+            hi = (uint64_t)v.z | ((uint64_t)v.w << 32);
+        } else {
+            for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+            for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        }
         uint16_t h[48];
         decode_bc6h_block_u(lo, hi, h);
+#pragma unroll
         for (int y = 0; y < 4; y++) {
             size_t row = (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
             if (fmt == 0) {
                 uint8_t* o = reinterpret_cast<uint8_t*>(out) + row;
+                uint32_t px[4];
+#pragma unroll
                 for (int x = 0; x < 4; x++) {
-                    for (int c = 0; c < 3; c++) o[4 * x + c] = g_half_to_srgb[min((int)h[(y * 4 + x) * 3 + c], 0x7BFF)];
-                    o[4 * x + 3] = 0;
+                    px[x] = 0;
+#pragma unroll
+                    for (int c = 0; c < 3; c++)
+                        px[x] |= (uint32_t)__ldg(&g_half_to_srgb[min((int)h[(y * 4 + x) * 3 + c], 0x7BFF)]) << (8 * c);
+                }
+                if (aligned) {
+                    *reinterpret_cast<uint4*>(o) = make_uint4(px[0], px[1], px[2], px[3]);
+                } else {
+                    for (int j = 0; j < 16; j++) o[j] = (uint8_t)(px[j >> 2] >> (8 * (j & 3)));
                 }
             } else if (fmt == 1) {
                 uint16_t* o = reinterpret_cast<uint16_t*>(out) + row;
-                for (int j = 0; j < 12; j++) o[j] = h[y * 12 + j];
+                if (aligned) {
+                    uint32_t w[6];
+#pragma unroll
+                    for (int j = 0; j < 6; j++) w[j] = (uint32_t)h[y * 12 + 2 * j] | ((uint32_t)h[y * 12 + 2 * j + 1] << 16);
+                    uint2* o2 = reinterpret_cast<uint2*>(o);
+                    o2[0] = make_uint2(w[0], w[1]);
+                    o2[1] = make_uint2(w[2], w[3]);
+                    o2[2] = make_uint2(w[4], w[5]);
+                } else {
+                    for (int j = 0; j < 12; j++) o[j] = h[y * 12 + j];
+                }
             } else {
                 float* o = reinterpret_cast<float*>(out) + row;
-                for (int j = 0; j < 12; j++) o[j] = __half2float(__ushort_as_half(h[y * 12 + j]));
+                float f[12];
+#pragma unroll
+                for (int j = 0; j < 12; j++) f[j] = __half2float(__ushort_as_half(h[y * 12 + j]));
+                if (aligned) {
+                    float4* o4 = reinterpret_cast<float4*>(o);
+                    o4[0] = make_float4(f[0], f[1], f[2], f[3]);
+                    o4[1] = make_float4(f[4], f[5], f[6], f[7]);
+                    o4[2] = make_float4(f[8], f[9], f[10], f[11]);
+                } else {
+                    for (int j = 0; j < 12; j++) o[j] = f[j];
+                }
             }
         }
     }
@@ -280,7 +328,11 @@ void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t*
 void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
                         cudaStream_t s) {
     if (bw == 0 || bh == 0) return;
-    bc6h_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, out_format);
+    // aligned: 16-byte block loads, and row stores of 16 B (RGBA8), 8 B
+    // (RGBA16F, rows start at 32-byte multiples) or 16 B (RGBA32F)
+    size_t esize = out_format == 0 ? 1 : (out_format == 1 ? 2 : 4);
+    bool aligned = ((uintptr_t)blocks % 16 == 0) && ((uintptr_t)out % 16 == 0) && ((pitch * esize) % 16 == 0);
+    bc6h_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, out_format, aligned);
 }
 
 }  // namespace bcn

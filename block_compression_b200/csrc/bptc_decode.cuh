@@ -44,140 +44,167 @@ BCN_DEV int w_of(int bits, int i) {
 }
 
 // ---- BC7 (block.rs:801-1252) --------------------------------------------------
+//
+// One decoder per mode: every field of a mode sits at a fixed bit position,
+// so a mode compiles to straight-line funnel shifts. The index bits are read
+// as one bit string in which a zero is re-inserted above each anchor index
+// (anchors are stored one bit short); pixel k's index is then at bits
+// [k*IB, k*IB + IB). Interpolation runs on two channels at once in 16-bit
+// lanes: (e0 * (64 - w) + e1 * w + 32) >> 6 stays below 2^16 per lane.
+
+// Partition tables in global memory: the lanes of a warp read different
+// partitions, which the constant cache would serialise.
+__device__ const uint32_t kDecPartitionMap[128] = {BCN_PARTITION_MAP_VALUES};
+__device__ const uint8_t kDecAnchors[128] = {BCN_ANCHOR_VALUES};
+
+// n <= 32 bits at bit `pos` of the block (d[4] = 0 pads the end).
+BCN_DEV uint32_t bits_at(const uint32_t d[5], int pos, int n) {
+    uint32_t v = __funnelshift_r(d[pos >> 5], d[(pos >> 5) + 1], pos & 31);
+    return n == 32 ? v : (v & ((1u << n) - 1u));
+}
+
+// Up to 64 bits from bit `pos`, zero past bit 127.
+BCN_DEV uint64_t bits64_at(const uint32_t d[5], int pos) {
+    int w = pos >> 5, s = pos & 31;
+    uint32_t x2 = w + 2 < 5 ? d[w + 2] : 0u;
+    uint32_t lo = __funnelshift_r(d[w], d[w + 1], s), hi = __funnelshift_r(d[w + 1], x2, s);
+    return (uint64_t)lo | ((uint64_t)hi << 32);
+}
+
+BCN_DEV uint64_t insert_zero(uint64_t x, uint32_t p) {
+    uint64_t m = (1ull << p) - 1ull;
+    return (x & m) | ((x & ~m) << 1);
+}
+
+// Bit replication of a P-bit value to 8 bits.
+template <int P>
+BCN_DEV uint32_t expand8(uint32_t v) {
+    if constexpr (P >= 8) return v;
+    else if constexpr (P >= 4) return (v << (8 - P)) | (v >> (2 * P - 8));
+    else return v;  // never instantiated for a decoded field (P >= 4 in every mode)
+}
+
+// BPTC index weights (0..64) of 2-, 3- and 4-bit indices, as byte tables.
+template <int IB>
+BCN_DEV uint32_t bptc_weight(uint32_t i) {
+    if (IB == 2) return __byte_perm(0x402B1500u, 0u, i) & 0xFFu;
+    if (IB == 3) return __byte_perm(0x1B120900u, 0x40372E25u, i) & 0xFFu;
+    uint32_t lo = __byte_perm(0x0D090400u, 0x1E1A1511u, i & 7u), hi = __byte_perm(0x2F2B2622u, 0x403C3733u, i & 7u);
+    return ((i & 8u) ? hi : lo) & 0xFFu;
+}
+
+// Two 8-bit channels in 16-bit lanes, interpolated with one weight.
+BCN_DEV uint32_t lerp2(uint32_t e0, uint32_t e1, uint32_t w) { return (e0 * (64u - w) + e1 * w + 0x00200020u) >> 6; }
+
+template <int MODE>
+BCN_DEV void decode_bc7_mode(const uint32_t d[5], uint32_t out[16]) {
+    constexpr int NS = (MODE == 0 || MODE == 2) ? 3 : ((MODE == 1 || MODE == 3 || MODE == 7) ? 2 : 1);
+    constexpr int NEP = 2 * NS;
+    constexpr int PB = MODE == 0 ? 4 : (NS > 1 ? 6 : 0);
+    constexpr int CB = MODE == 0 ? 4 : (MODE == 1 ? 6 : (MODE == 2 || MODE == 4 || MODE == 7) ? 5 : 7);
+    constexpr int AB = MODE == 4 ? 6 : (MODE == 5 ? 8 : (MODE == 6 ? 7 : (MODE == 7 ? 5 : 0)));
+    constexpr int PBT = (MODE == 0 || MODE == 3 || MODE == 6 || MODE == 7) ? 1 : (MODE == 1 ? 2 : 0);
+    constexpr int IB = (MODE == 0 || MODE == 1) ? 3 : (MODE == 6 ? 4 : 2);
+    constexpr int IB2 = MODE == 4 ? 3 : (MODE == 5 ? 2 : 0);
+    constexpr int HDR = MODE + 1 + PB + ((MODE == 4 || MODE == 5) ? 2 : 0) + (MODE == 4 ? 1 : 0);
+    constexpr int PP = HDR + 3 * NEP * CB + NEP * AB;
+    constexpr int IS = PP + (PBT == 1 ? NEP : (PBT == 2 ? 2 : 0));
+    constexpr int T1 = 16 * IB - NS;
+    constexpr int PC = CB + (PBT ? 1 : 0), PA = AB + (PBT ? 1 : 0);
+
+    uint32_t part = PB ? bits_at(d, MODE + 1, PB) : 0u;
+    uint32_t rot = 0, isb = 0;
+    if (MODE == 4 || MODE == 5) rot = bits_at(d, MODE + 1, 2);
+    if (MODE == 4) isb = bits_at(d, MODE + 3, 1);
+    uint32_t erg[NEP], eba[NEP];
+#pragma unroll
+    for (int j = 0; j < NEP; j++) {
+        uint32_t pb = PBT == 1 ? bits_at(d, PP + j, 1) : (PBT == 2 ? bits_at(d, PP + (j >> 1), 1) : 0u);
+        uint32_t c[3];
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) {
+            uint32_t v = bits_at(d, HDR + (ch * NEP + j) * CB, CB);
+            c[ch] = expand8<PC>(PBT ? ((v << 1) | pb) : v);
+        }
+        uint32_t a = 255u;
+        if constexpr (AB > 0) {
+            uint32_t v = bits_at(d, HDR + 3 * NEP * CB + j * AB, AB);
+            a = expand8<PA>(PBT ? ((v << 1) | pb) : v);
+        }
+        erg[j] = c[0] | (c[1] << 16);
+        eba[j] = c[2] | (a << 16);
+    }
+    uint32_t table = NS == 3 ? 64u + part : part;
+    uint32_t map = NS > 1 ? __ldg(&kDecPartitionMap[table]) : 0u;
+    uint64_t x = bits64_at(d, IS);
+    if constexpr (T1 < 64) x &= (1ull << T1) - 1ull;
+    x = insert_zero(x, IB - 1);
+    if (NS == 2) {
+        uint32_t a1 = __ldg(&kDecAnchors[table]) >> 4;
+        x = insert_zero(x, a1 * IB + IB - 1);
+    } else if (NS == 3) {
+        uint32_t an = __ldg(&kDecAnchors[table]);
+        uint32_t a1 = an >> 4, a2 = an & 15u;
+        uint32_t lo = a1 < a2 ? a1 : a2, hi = a1 < a2 ? a2 : a1;
+        x = insert_zero(x, lo * IB + IB - 1);
+        x = insert_zero(x, hi * IB + IB - 1);
+    }
+    uint64_t y = 0;
+    if constexpr (IB2 > 0) {
+        y = bits64_at(d, IS + T1) & ((1ull << (16 * IB2 - 1)) - 1ull);
+        y = insert_zero(y, IB2 - 1);
+    }
+    // rotation: swap alpha with R (1), G (2) or B (3)
+    const uint32_t rot_sel = rot == 1 ? 0x0213u : (rot == 2 ? 0x1230u : (rot == 3 ? 0x2310u : 0x3210u));
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        uint32_t s = NS > 1 ? ((map >> (2 * k)) & 3u) : 0u;
+        uint32_t e0rg = erg[0], e1rg = erg[1], e0ba = eba[0], e1ba = eba[1];
+        if (NS > 1 && s == 1) {
+            e0rg = erg[2];
+            e1rg = erg[3];
+            e0ba = eba[2];
+            e1ba = eba[3];
+        }
+        if (NS > 2 && s == 2) {
+            e0rg = erg[NEP > 4 ? 4 : 0];
+            e1rg = erg[NEP > 5 ? 5 : 1];
+            e0ba = eba[NEP > 4 ? 4 : 0];
+            e1ba = eba[NEP > 5 ? 5 : 1];
+        }
+        uint32_t w1 = bptc_weight<IB>((uint32_t)(x >> (k * IB)) & ((1u << IB) - 1u));
+        uint32_t px;
+        if constexpr (IB2 > 0) {
+            uint32_t w2 = bptc_weight<IB2>((uint32_t)(y >> (k * IB2)) & ((1u << IB2) - 1u));
+            uint32_t wc = isb ? w2 : w1, wa = isb ? w1 : w2;
+            uint32_t rg = lerp2(e0rg, e1rg, wc);
+            uint32_t lo = (e0ba & 0xFFFFu) * (64u - wc) + (e1ba & 0xFFFFu) * wc;
+            uint32_t hi = (e0ba >> 16) * (64u - wa) + (e1ba >> 16) * wa;
+            uint32_t ba = (lo + (hi << 16) + 0x00200020u) >> 6;
+            px = __byte_perm(__byte_perm(rg, ba, 0x6420u), 0u, rot_sel);
+        } else {
+            px = __byte_perm(lerp2(e0rg, e1rg, w1), lerp2(e0ba, e1ba, w1), 0x6420u);
+        }
+        out[k] = px;
+    }
+}
 
 BCN_DEV void decode_bc7_block(uint64_t lo, uint64_t hi, uint32_t out[16]) {
-    const uint32_t abits0 = 0x57757564u;  // RGB bits per mode, 4 bits each: 4,6,5,7,5,7,7,5
-    const uint32_t abits1 = 0x57860000u;  // alpha bits per mode: 0,0,0,0,6,8,7,5
-    const uint32_t has_pbits = 0xCB;
-    Bits128 bs{lo, hi};
-    uint32_t mode = 0;
-    while (mode < 8 && bs.read(1) == 0) mode++;
-    if (mode >= 8) {
-        for (int k = 0; k < 16; k++) out[k] = 0;
-        return;
-    }
-    uint32_t cbits = (abits0 >> (4 * mode)) & 15, abits = (abits1 >> (4 * mode)) & 15;
-    uint32_t partition = 0, nparts = 1, rotation = 0, isb = 0;
-    if (mode == 0 || mode == 1 || mode == 2 || mode == 3 || mode == 7) {
-        nparts = (mode == 0 || mode == 2) ? 3 : 2;
-        partition = bs.read(mode == 0 ? 4 : 6);
-    }
-    uint32_t nep = nparts * 2;
-    if (mode == 4 || mode == 5) {
-        rotation = bs.read(2);
-        if (mode == 4) isb = bs.read(1);
-    }
-    int ep[6][4];
+    const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
+    uint32_t low = d[0] & 0xFFu;
+    int mode = low ? __ffs((int)low) - 1 : 8;
+    switch (mode) {
+        case 0: decode_bc7_mode<0>(d, out); break;
+        case 1: decode_bc7_mode<1>(d, out); break;
+        case 2: decode_bc7_mode<2>(d, out); break;
+        case 3: decode_bc7_mode<3>(d, out); break;
+        case 4: decode_bc7_mode<4>(d, out); break;
+        case 5: decode_bc7_mode<5>(d, out); break;
+        case 6: decode_bc7_mode<6>(d, out); break;
+        case 7: decode_bc7_mode<7>(d, out); break;
+        default:
 #pragma unroll
-    for (int j = 0; j < 6; j++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) ep[j][c] = 0;
-    for (int c = 0; c < 3; c++)
-        for (uint32_t j = 0; j < nep; j++) {
-            int v = (int)bs.read(cbits);
-#pragma unroll
-            for (int jj = 0; jj < 6; jj++)
-                if (jj == (int)j) ep[jj][c] = v;
-        }
-    if (abits > 0)
-        for (uint32_t j = 0; j < nep; j++) {
-            int v = (int)bs.read(abits);
-#pragma unroll
-            for (int jj = 0; jj < 6; jj++)
-                if (jj == (int)j) ep[jj][3] = v;
-        }
-    uint32_t pb = (has_pbits >> mode) & 1;
-    if (mode == 0 || mode == 1 || mode == 3 || mode == 6 || mode == 7) {
-#pragma unroll
-        for (int j = 0; j < 6; j++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) ep[j][c] <<= 1;
-        if (mode == 1) {
-            int i0 = (int)bs.read(1), j0 = (int)bs.read(1);
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                ep[0][c] |= i0;
-                ep[1][c] |= i0;
-                ep[2][c] |= j0;
-                ep[3][c] |= j0;
-            }
-        } else if (pb) {
-            for (uint32_t j = 0; j < nep; j++) {
-                int b = (int)bs.read(1);
-#pragma unroll
-                for (int jj = 0; jj < 6; jj++)
-                    if (jj == (int)j)
-#pragma unroll
-                        for (int c = 0; c < 4; c++) ep[jj][c] |= b;
-            }
-        }
-    }
-    {
-        uint32_t jc = cbits + pb, ja = abits + pb;
-#pragma unroll
-        for (int j = 0; j < 6; j++) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                ep[j][c] <<= 8 - jc;
-                ep[j][c] |= ep[j][c] >> jc;
-            }
-            ep[j][3] <<= 8 - ja;
-            ep[j][3] |= ep[j][3] >> ja;
-            if (abits == 0) ep[j][3] = 0xFF;
-        }
-    }
-    uint32_t ib = (mode == 0 || mode == 1) ? 3 : (mode == 6 ? 4 : 2);
-    uint32_t ib2 = mode == 4 ? 3 : (mode == 5 ? 2 : 0);
-    uint32_t table = nparts == 3 ? 64 + partition : partition;
-    uint32_t idx[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        uint32_t ps = nparts == 1 ? (k == 0 ? 0x80u : 0u) : partition_set(table, k);
-        idx[k] = bs.read((ps & 0x80) ? ib - 1 : ib);
-    }
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-        uint32_t s = nparts == 1 ? 0u : (partition_set(table, k) & 3);
-        const int* e0 = s == 0 ? ep[0] : (s == 1 ? ep[2] : ep[4]);
-        const int* e1 = s == 0 ? ep[1] : (s == 1 ? ep[3] : ep[5]);
-        int r, g, b, a;
-        int w = w_of((int)ib, (int)idx[k]);
-        if (ib2 == 0) {
-            r = interp(e0[0], e1[0], w);
-            g = interp(e0[1], e1[1], w);
-            b = interp(e0[2], e1[2], w);
-            a = interp(e0[3], e1[3], w);
-        } else {
-            int i2 = (int)bs.read(k == 0 ? ib2 - 1 : ib2);
-            int w2 = w_of((int)ib2, i2);
-            if (isb == 0) {
-                r = interp(e0[0], e1[0], w);
-                g = interp(e0[1], e1[1], w);
-                b = interp(e0[2], e1[2], w);
-                a = interp(e0[3], e1[3], w2);
-            } else {
-                r = interp(e0[0], e1[0], w2);
-                g = interp(e0[1], e1[1], w2);
-                b = interp(e0[2], e1[2], w2);
-                a = interp(e0[3], e1[3], w);
-            }
-        }
-        int t;
-        if (rotation == 1) {
-            t = a;
-            a = r;
-            r = t;
-        } else if (rotation == 2) {
-            t = a;
-            a = g;
-            g = t;
-        } else if (rotation == 3) {
-            t = a;
-            a = b;
-            b = t;
-        }
-        out[k] = (uint32_t)(r & 0xFF) | ((uint32_t)(g & 0xFF) << 8) | ((uint32_t)(b & 0xFF) << 16) |
-                 ((uint32_t)(a & 0xFF) << 24);
+            for (int k = 0; k < 16; k++) out[k] = 0u;
     }
 }
 }  // namespace bcn
