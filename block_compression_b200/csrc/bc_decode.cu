@@ -15,32 +15,150 @@
 namespace bcn {
 
 
+// Mode-sorted BC7 decode. Neighbouring blocks often use different modes, and
+// the per-mode decoders diverge inside a warp. A CTA therefore takes 256
+// consecutive blocks, sorts them by mode in shared memory (counting sort),
+// decodes them in sorted order -- so a warp mostly runs one mode's code --
+// and puts the texels back in image order in shared memory, from where the
+// 4 texel rows of each block are written with coalesced 16-byte stores.
+constexpr int kSortCta = 256;
+
+// Counting-sort rank of this thread's key among the CTA's 256 keys (keys <
+// nkeys <= 32). Lanes with equal keys are counted once per warp
+// (__match_any_sync), so each warp makes at most one shared-memory atomic
+// per distinct key. s_cnt must hold 32 words.
+BCN_DEV uint32_t cta_sort_slot(uint32_t key, uint32_t nkeys, uint32_t* s_cnt) {
+    const uint32_t t = threadIdx.x, lane = t & 31u;
+    if (t < 32) s_cnt[t] = 0;
+    __syncthreads();
+    uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+    uint32_t leader = __ffs((int)peers) - 1u;
+    uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t wbase = 0;
+    if (lane == leader) wbase = atomicAdd(&s_cnt[key], (uint32_t)__popc(peers));
+    wbase = __shfl_sync(0xFFFFFFFFu, wbase, (int)leader);
+    __syncthreads();
+    if (t < 32) {  // exclusive prefix sum of the counts over the first warp
+        uint32_t c = t < nkeys ? s_cnt[t] : 0u, x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        s_cnt[t] = x - c;
+    }
+    __syncthreads();
+    return s_cnt[key] + wbase + rank;
+}
+
+// Mode-sorted BC7 decode, 4 blocks per thread: a CTA sorts 1024 consecutive
+// blocks by mode in shared memory and decodes them in sorted order, so a
+// warp mostly runs one mode's code; each thread writes its decoded block's 4
+// texel rows (16 B each) straight to the image. Groups whose warps already
+// hold one mode each skip the sort.
+constexpr int kSortItems = 4;
+
+__global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8_t* __restrict__ blocks, uint32_t bw,
+                                                                     uint32_t bh, uint8_t* __restrict__ out,
+                                                                     size_t pitch) {
+    constexpr uint32_t G = kSortCta * kSortItems;
+    __shared__ uint4 s_blk[G];
+    __shared__ uint32_t s_orig[G];
+    __shared__ uint32_t s_cnt[32];
+    const uint32_t n = bw * bh, t = threadIdx.x, lane = t & 31u;
+    const uint32_t stride = gridDim.x * G;
+    for (uint32_t base = blockIdx.x * G; base < n; base += stride) {
+        uint4 v[kSortItems];
+        uint32_t key[kSortItems];
+        bool uniform = true;
+#pragma unroll
+        for (int q = 0; q < kSortItems; q++) {
+            uint32_t i = base + q * kSortCta + t;
+            v[q] = i < n ? __ldg(reinterpret_cast<const uint4*>(blocks) + i) : make_uint4(0u, 0u, 0u, 0u);
+            uint32_t low = v[q].x & 0xFFu;
+            key[q] = low ? (uint32_t)__ffs((int)low) - 1u : 8u;
+            uniform &= __all_sync(0xFFFFFFFFu, key[q] == __shfl_sync(0xFFFFFFFFu, key[q], 0));
+        }
+        if (__syncthreads_and(uniform)) {
+#pragma unroll
+            for (int q = 0; q < kSortItems; q++) {
+                uint32_t i = base + q * kSortCta + t;
+                if (i >= n) continue;
+                uint32_t px[16];
+                decode_bc7_block((uint64_t)v[q].x | ((uint64_t)v[q].y << 32), (uint64_t)v[q].z | ((uint64_t)v[q].w << 32), px);
+                uint32_t by = i / bw, bx = i - by * bw;
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+                    *reinterpret_cast<uint4*>(out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16) =
+                        make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+            }
+            continue;
+        }
+        // counting sort of the G keys (warp-aggregated shared-memory atomics)
+        if (t < 32) s_cnt[t] = 0;
+        __syncthreads();
+        uint32_t wpos[kSortItems];
+#pragma unroll
+        for (int q = 0; q < kSortItems; q++) {
+            uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[q]);
+            uint32_t leader = __ffs((int)peers) - 1u;
+            uint32_t b = 0;
+            if (lane == leader) b = atomicAdd(&s_cnt[key[q]], (uint32_t)__popc(peers));
+            wpos[q] = __shfl_sync(0xFFFFFFFFu, b, (int)leader) + __popc(peers & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        if (t < 32) {
+            uint32_t c = t < 9 ? s_cnt[t] : 0u, x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= (uint32_t)o) x += y;
+            }
+            s_cnt[t] = x - c;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kSortItems; q++) {
+            uint32_t slot = s_cnt[key[q]] + wpos[q];
+            s_blk[slot] = v[q];
+            s_orig[slot] = base + q * kSortCta + t;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kSortItems; q++) {
+            uint4 b = s_blk[q * kSortCta + t];
+            uint32_t i = s_orig[q * kSortCta + t];
+            if (i < n) {
+                uint32_t px[16];
+                decode_bc7_block((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), px);
+                uint32_t by = i / bw, bx = i - by * bw;
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+                    *reinterpret_cast<uint4*>(out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16) =
+                        make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+            }
+        }
+        __syncthreads();  // s_blk / s_orig / s_cnt are reused by the next group
+    }
+}
+
+// Unaligned buffers: one thread per block, byte loads and stores.
 __global__ void __launch_bounds__(128) bc7_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
-                                                         uint8_t* __restrict__ out, size_t pitch, bool aligned) {
+                                                         uint8_t* __restrict__ out, size_t pitch) {
     uint32_t n = bw * bh;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t by = i / bw, bx = i - by * bw;
         uint64_t lo = 0, hi = 0;
         const uint8_t* b = blocks + (size_t)i * 16;
-        if (aligned) {
-            uint4 v = __ldg(reinterpret_cast<const uint4*>(b));
-            lo = (uint64_t)v.x | ((uint64_t)v.y << 32);
-            hi = (uint64_t)v.z | ((uint64_t)v.w << 32);
-        } else {
-            for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
-            for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
-        }
+        for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+        for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
         uint32_t px[16];
         decode_bc7_block(lo, hi, px);
 #pragma unroll
         for (int y = 0; y < 4; y++) {
             uint8_t* row = out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
-            if (aligned) {
-                *reinterpret_cast<uint4*>(row) = make_uint4(px[y * 4], px[y * 4 + 1], px[y * 4 + 2], px[y * 4 + 3]);
-            } else {
-                for (int x = 0; x < 4; x++)
-                    for (int c = 0; c < 4; c++) row[4 * x + c] = (uint8_t)(px[y * 4 + x] >> (8 * c));
-            }
+            for (int x = 0; x < 4; x++)
+                for (int c = 0; c < 4; c++) row[4 * x + c] = (uint8_t)(px[y * 4 + x] >> (8 * c));
         }
     }
 }
@@ -58,14 +176,33 @@ BCN_DEV int unquantize_u(int v, int bits) {
 
 // Unsigned BC6H (the only form the image drivers use): 16 pixels of RGB
 // f16 bit patterns.
-BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
-    Bits128 bs{lo, hi};
+// LSB-first reader over the block at a position the compiler can track: each
+// mode's case sets the start position and reads fixed widths, so every field
+// resolves to a fixed bit offset (funnel shifts, no 128-bit shifting).
+struct PosBits {
+    const uint32_t* d;  // 5 words, d[4] = 0
+    int p;
+    BCN_DEV uint32_t read(int n) {
+        uint32_t v = bits_at(d, p, n);
+        p += n;
+        return v;
+    }
+    BCN_DEV int ri(int n) { return (int)read(n); }
+    BCN_DEV int rev(int n) { return (int)(__brev(read(n)) >> (32 - n)); }
+};
+
+// Output: 48 f16 bit patterns (pixel k's RGB at elements 3k..3k+2), packed
+// two per word: element e in bits 16 * (e & 1) of out[e >> 1].
+BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint32_t out[24]) {
+    const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
+    PosBits bs{d, 0};
     int r[4] = {0, 0, 0, 0}, g[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
     uint32_t mode = bs.read(2);
     if (mode > 1) mode |= bs.read(3) << 2;
     int part = 0;
     switch (mode) {
         case 0x00:
+            bs.p = 2;
             g[2] |= bs.ri(1) << 4; b[2] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 4;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
@@ -75,6 +212,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 0;
             break;
         case 0x01:
+            bs.p = 2;
             g[2] |= bs.ri(1) << 5; g[3] |= bs.ri(1) << 4; g[3] |= bs.ri(1) << 5;
             r[0] |= bs.ri(7); b[3] |= bs.ri(1); b[3] |= bs.ri(1) << 1;
             b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(7); b[2] |= bs.ri(1) << 5;
@@ -85,6 +223,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             r[2] |= bs.ri(6); r[3] |= bs.ri(6); part = bs.ri(5); mode = 1;
             break;
         case 0x02:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(5); r[0] |= bs.ri(1) << 10; g[2] |= bs.ri(4);
             g[1] |= bs.ri(4); g[0] |= bs.ri(1) << 10; b[3] |= bs.ri(1);
@@ -94,6 +233,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             part = bs.ri(5); mode = 2;
             break;
         case 0x06:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(4); r[0] |= bs.ri(1) << 10; g[3] |= bs.ri(1) << 4;
             g[2] |= bs.ri(4); g[1] |= bs.ri(5); g[0] |= bs.ri(1) << 10;
@@ -103,6 +243,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             g[2] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 3;
             break;
         case 0x0A:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(4); r[0] |= bs.ri(1) << 10; b[2] |= bs.ri(1) << 4;
             g[2] |= bs.ri(4); g[1] |= bs.ri(4); g[0] |= bs.ri(1) << 10;
@@ -112,6 +253,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             b[3] |= bs.ri(1) << 4; b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 4;
             break;
         case 0x0E:
+            bs.p = 5;
             r[0] |= bs.ri(9); b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(9);
             g[2] |= bs.ri(1) << 4; b[0] |= bs.ri(9); b[3] |= bs.ri(1) << 4;
             r[1] |= bs.ri(5); g[3] |= bs.ri(1) << 4; g[2] |= bs.ri(4);
@@ -121,6 +263,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             b[3] |= bs.ri(1) << 3; part = bs.ri(5); mode = 5;
             break;
         case 0x12:
+            bs.p = 5;
             r[0] |= bs.ri(8); g[3] |= bs.ri(1) << 4; b[2] |= bs.ri(1) << 4;
             g[0] |= bs.ri(8); b[3] |= bs.ri(1) << 2; g[2] |= bs.ri(1) << 4;
             b[0] |= bs.ri(8); b[3] |= bs.ri(1) << 3; b[3] |= bs.ri(1) << 4;
@@ -130,6 +273,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             r[3] |= bs.ri(6); part = bs.ri(5); mode = 6;
             break;
         case 0x16:
+            bs.p = 5;
             r[0] |= bs.ri(8); b[3] |= bs.ri(1); b[2] |= bs.ri(1) << 4;
             g[0] |= bs.ri(8); g[2] |= bs.ri(1) << 5; g[2] |= bs.ri(1) << 4;
             b[0] |= bs.ri(8); g[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
@@ -140,6 +284,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             part = bs.ri(5); mode = 7;
             break;
         case 0x1A:
+            bs.p = 5;
             r[0] |= bs.ri(8); b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(1) << 4;
             g[0] |= bs.ri(8); b[2] |= bs.ri(1) << 5; g[2] |= bs.ri(1) << 4;
             b[0] |= bs.ri(8); b[3] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 4;
@@ -150,6 +295,7 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             part = bs.ri(5); mode = 8;
             break;
         case 0x1E:
+            bs.p = 5;
             r[0] |= bs.ri(6); g[3] |= bs.ri(1) << 4; b[3] |= bs.ri(1);
             b[3] |= bs.ri(1) << 1; b[2] |= bs.ri(1) << 4; g[0] |= bs.ri(6);
             g[2] |= bs.ri(1) << 5; b[2] |= bs.ri(1) << 5; b[3] |= bs.ri(1) << 2;
@@ -160,44 +306,53 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
             r[2] |= bs.ri(6); r[3] |= bs.ri(6); part = bs.ri(5); mode = 9;
             break;
         case 0x03:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(10); g[1] |= bs.ri(10); b[1] |= bs.ri(10);
             mode = 10;
             break;
         case 0x07:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(9); r[0] |= bs.ri(1) << 10; g[1] |= bs.ri(9);
             g[0] |= bs.ri(1) << 10; b[1] |= bs.ri(9); b[0] |= bs.ri(1) << 10;
             mode = 11;
             break;
         case 0x0B:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(8); r[0] |= bs.rev(2) << 10; g[1] |= bs.ri(8);
             g[0] |= bs.rev(2) << 10; b[1] |= bs.ri(8); b[0] |= bs.rev(2) << 10;
             mode = 12;
             break;
         case 0x0F:
+            bs.p = 5;
             r[0] |= bs.ri(10); g[0] |= bs.ri(10); b[0] |= bs.ri(10);
             r[1] |= bs.ri(4); r[0] |= bs.rev(6) << 10; g[1] |= bs.ri(4);
             g[0] |= bs.rev(6) << 10; b[1] |= bs.ri(4); b[0] |= bs.rev(6) << 10;
             mode = 13;
             break;
         default:
-            for (int i = 0; i < 48; i++) out[i] = 0;
+#pragma unroll
+            for (int i = 0; i < 24; i++) out[i] = 0;
             return;
     }
-    // ACTUAL_BITS_COUNT (block.rs:269-274)
-    const uint8_t kB0[14] = {10, 7, 11, 11, 11, 9, 8, 8, 8, 6, 10, 11, 12, 16};
-    const uint8_t kBR[14] = {5, 6, 5, 4, 4, 5, 6, 5, 5, 6, 10, 9, 8, 4};
-    const uint8_t kBG[14] = {5, 6, 4, 5, 4, 5, 5, 6, 5, 6, 10, 9, 8, 4};
-    const uint8_t kBB[14] = {5, 6, 4, 4, 5, 5, 5, 5, 6, 6, 10, 9, 8, 4};
+    // ACTUAL_BITS_COUNT (block.rs:269-274), one byte per mode in two words:
+    // endpoint bits {10, 7, 11, 11, 11, 9, 8, 8, 8, 6, 10, 11, 12, 16} and the
+    // delta bits of R, G and B.
+    auto tab14 = [mode](uint64_t lo, uint64_t hi) {
+        return (int)(((mode < 8 ? lo >> (8 * mode) : hi >> (8 * (mode - 8)))) & 0xFFu);
+    };
     int np = mode >= 10 ? 0 : 1;
-    int bits0 = kB0[mode];
+    int bits0 = tab14(0x0808090B0B0B070AULL, 0x100C0B0A0608ULL);
+    const int br = tab14(0x0506050404050605ULL, 0x0408090A0605ULL);
+    const int bgb = tab14(0x0605050405040605ULL, 0x0408090A0605ULL);
+    const int bbb = tab14(0x0505050504040605ULL, 0x0408090A0606ULL);
     if (mode != 9 && mode != 10) {
         for (int i = 1; i < (np + 1) * 2; i++) {
-            int rr = extend_sign(i == 1 ? r[1] : (i == 2 ? r[2] : r[3]), kBR[mode]);
-            int gg = extend_sign(i == 1 ? g[1] : (i == 2 ? g[2] : g[3]), kBG[mode]);
-            int bb = extend_sign(i == 1 ? b[1] : (i == 2 ? b[2] : b[3]), kBB[mode]);
+            int rr = extend_sign(i == 1 ? r[1] : (i == 2 ? r[2] : r[3]), br);
+            int gg = extend_sign(i == 1 ? g[1] : (i == 2 ? g[2] : g[3]), bgb);
+            int bb = extend_sign(i == 1 ? b[1] : (i == 2 ? b[2] : b[3]), bbb);
             int m = (1 << bits0) - 1;
             rr = (rr + r[0]) & m;
             gg = (gg + g[0]) & m;
@@ -217,7 +372,6 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
     // Index bits: 46 bits from bit 82 (two subsets, 3-bit indices) or 63 bits
     // from bit 65 (one subset, 4-bit); a zero is re-inserted above each anchor
     // index so that pixel k's index sits at bits [k*ib, k*ib + ib).
-    const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
     uint32_t map = 0;
     uint64_t x;
     if (mode >= 10) {
@@ -237,9 +391,14 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
         int r0 = e ? r[2] : r[0], r1 = e ? r[3] : r[1];
         int g0 = e ? g[2] : g[0], g1 = e ? g[3] : g[1];
         int b0 = e ? b[2] : b[0], b1 = e ? b[3] : b[1];
-        out[k * 3 + 0] = (uint16_t)((interp(r0, r1, w) * 31) >> 6);
-        out[k * 3 + 1] = (uint16_t)((interp(g0, g1, w) * 31) >> 6);
-        out[k * 3 + 2] = (uint16_t)((interp(b0, b1, w) * 31) >> 6);
+        const uint32_t c[3] = {(uint32_t)((interp(r0, r1, w) * 31) >> 6), (uint32_t)((interp(g0, g1, w) * 31) >> 6),
+                               (uint32_t)((interp(b0, b1, w) * 31) >> 6)};
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) {
+            const int e = k * 3 + ch;
+            if (e & 1) out[e >> 1] |= c[ch] << 16;
+            else out[e >> 1] = c[ch];
+        }
     }
 }
 
@@ -248,67 +407,129 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint16_t out[48]) {
 // evaluated on the host for every such bit pattern.
 __device__ uint8_t g_half_to_srgb[0x7C00];
 
+// BC6H mode key of a block for the mode sort: 0/1 for the 2-bit mode
+// prefixes, 2 + (bits 2..4) (+8 when bit 0 is set) for the 5-bit ones.
+BCN_DEV uint32_t bc6h_mode_key(uint32_t b0) {
+    uint32_t p = b0 & 31u;
+    if ((p & 3u) < 2u) return p & 3u;
+    return 2u + ((p >> 2) & 7u) + ((p & 1u) ? 8u : 0u);
+}
+
+// Writes row y of one decoded block (12 f16 elements: 6 packed words) in the
+// output format: 0 RGBA8 via linear_to_srgb with A = 0, 1 RGBA16F RGB
+// triplets, 2 RGBA32F RGB triplets (the reference's layouts).
+BCN_DEV void bc6h_store_row(void* out, size_t row, int fmt, const uint32_t w[6]) {
+    if (fmt == 0) {
+        uint32_t px[4];
+#pragma unroll
+        for (int x = 0; x < 4; x++) {
+            px[x] = 0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int e = x * 3 + c;
+                uint32_t h = (w[e >> 1] >> (16 * (e & 1))) & 0xFFFFu;
+                px[x] |= (uint32_t)__ldg(&g_half_to_srgb[min((int)h, 0x7BFF)]) << (8 * c);
+            }
+        }
+        *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(out) + row) = make_uint4(px[0], px[1], px[2], px[3]);
+    } else if (fmt == 1) {
+        uint2* o2 = reinterpret_cast<uint2*>(reinterpret_cast<uint16_t*>(out) + row);
+        o2[0] = make_uint2(w[0], w[1]);
+        o2[1] = make_uint2(w[2], w[3]);
+        o2[2] = make_uint2(w[4], w[5]);
+    } else {
+        float f[12];
+#pragma unroll
+        for (int e = 0; e < 12; e++) f[e] = __half2float(__ushort_as_half((uint16_t)(w[e >> 1] >> (16 * (e & 1)))));
+        float4* o4 = reinterpret_cast<float4*>(reinterpret_cast<float*>(out) + row);
+        o4[0] = make_float4(f[0], f[1], f[2], f[3]);
+        o4[1] = make_float4(f[4], f[5], f[6], f[7]);
+        o4[2] = make_float4(f[8], f[9], f[10], f[11]);
+    }
+}
+
+// Mode-sorted BC6H decode (the scheme of bc7_decode_sorted_kernel): 256
+// blocks per CTA sorted by mode in shared memory, decoded in sorted order,
+// texels put back in image order in shared memory, rows written coalesced.
+__global__ void __launch_bounds__(kSortCta) bc6h_decode_sorted_kernel(const uint8_t* __restrict__ blocks, uint32_t bw,
+                                                                      uint32_t bh, void* __restrict__ out, size_t pitch,
+                                                                      int fmt) {
+    __shared__ uint4 s_blk[kSortCta];
+    __shared__ uint32_t s_out[24 * kSortCta];  // word q of local block t at [q * kSortCta + t]
+    __shared__ uint16_t s_orig[kSortCta];
+    __shared__ uint32_t s_cnt[32];
+    const uint32_t n = bw * bh, t = threadIdx.x;
+    const uint32_t stride = gridDim.x * kSortCta;
+    uint32_t base = blockIdx.x * kSortCta;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (base + t < n) v = __ldg(reinterpret_cast<const uint4*>(blocks) + base + t);
+    for (; base < n; base += stride) {
+        uint4 nv = make_uint4(0u, 0u, 0u, 0u);
+        if (base + stride + t < n) nv = __ldg(reinterpret_cast<const uint4*>(blocks) + base + stride + t);
+        uint32_t key = bc6h_mode_key(v.x);
+        bool uniform = __all_sync(0xFFFFFFFFu, key == __shfl_sync(0xFFFFFFFFu, key, 0));
+        if (__syncthreads_and(uniform)) {  // every warp already holds a single mode
+            uint32_t i = base + t;
+            if (i < n) {
+                uint32_t h[24];
+                decode_bc6h_block_u((uint64_t)v.x | ((uint64_t)v.y << 32), (uint64_t)v.z | ((uint64_t)v.w << 32), h);
+                uint32_t by = i / bw, bx = i - by * bw;
+#pragma unroll
+                for (int y = 0; y < 4; y++)
+                    bc6h_store_row(out, (size_t)(by * 4 + y) * pitch + (size_t)bx * 16, fmt, h + 6 * y);
+            }
+            v = nv;
+            continue;
+        }
+        uint32_t slot = cta_sort_slot(key, 18, s_cnt);
+        s_blk[slot] = v;
+        s_orig[slot] = (uint16_t)t;
+        __syncthreads();
+        uint4 b = s_blk[t];
+        uint32_t o = s_orig[t];
+        uint32_t h[24];
+        decode_bc6h_block_u((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), h);
+#pragma unroll
+        for (int q = 0; q < 24; q++) s_out[q * kSortCta + o] = h[q];
+        __syncthreads();
+        uint32_t i = base + t;
+        if (i < n) {
+            uint32_t by = i / bw, bx = i - by * bw;
+#pragma unroll
+            for (int y = 0; y < 4; y++) {
+                uint32_t w[6];
+#pragma unroll
+                for (int q = 0; q < 6; q++) w[q] = s_out[(y * 6 + q) * kSortCta + t];
+                bc6h_store_row(out, (size_t)(by * 4 + y) * pitch + (size_t)bx * 16, fmt, w);
+            }
+        }
+        v = nv;
+    }
+}
+
+// Unaligned buffers: one thread per block, byte/element loads and stores.
 __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
-                                                          void* __restrict__ out, size_t pitch, int fmt, bool aligned) {
+                                                          void* __restrict__ out, size_t pitch, int fmt) {
     uint32_t n = bw * bh;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t by = i / bw, bx = i - by * bw;
         const uint8_t* b = blocks + (size_t)i * 16;
         uint64_t lo = 0, hi = 0;
-        if (aligned) {
-            uint4 v = __ldg(reinterpret_cast<const uint4*>(b));
-            lo = (uint64_t)v.x | ((uint64_t)v.y << 32);
-            hi = (uint64_t)v.z | ((uint64_t)v.w << 32);
-        } else {
-            for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
-            for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
-        }
-        uint16_t h[48];
+        for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+        for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        uint32_t h[24];
         decode_bc6h_block_u(lo, hi, h);
-#pragma unroll
         for (int y = 0; y < 4; y++) {
             size_t row = (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
-            if (fmt == 0) {
-                uint8_t* o = reinterpret_cast<uint8_t*>(out) + row;
-                uint32_t px[4];
-#pragma unroll
-                for (int x = 0; x < 4; x++) {
-                    px[x] = 0;
-#pragma unroll
-                    for (int c = 0; c < 3; c++)
-                        px[x] |= (uint32_t)__ldg(&g_half_to_srgb[min((int)h[(y * 4 + x) * 3 + c], 0x7BFF)]) << (8 * c);
+            for (int x = 0; x < 4; x++) {
+                for (int c = 0; c < 3; c++) {
+                    const int e = (y * 4 + x) * 3 + c;
+                    uint16_t v = (uint16_t)(h[e >> 1] >> (16 * (e & 1)));
+                    if (fmt == 0) reinterpret_cast<uint8_t*>(out)[row + 4 * x + c] = g_half_to_srgb[min((int)v, 0x7BFF)];
+                    else if (fmt == 1) reinterpret_cast<uint16_t*>(out)[row + 3 * x + c] = v;
+                    else reinterpret_cast<float*>(out)[row + 3 * x + c] = __half2float(__ushort_as_half(v));
                 }
-                if (aligned) {
-                    *reinterpret_cast<uint4*>(o) = make_uint4(px[0], px[1], px[2], px[3]);
-                } else {
-                    for (int j = 0; j < 16; j++) o[j] = (uint8_t)(px[j >> 2] >> (8 * (j & 3)));
-                }
-            } else if (fmt == 1) {
-                uint16_t* o = reinterpret_cast<uint16_t*>(out) + row;
-                if (aligned) {
-                    uint32_t w[6];
-#pragma unroll
-                    for (int j = 0; j < 6; j++) w[j] = (uint32_t)h[y * 12 + 2 * j] | ((uint32_t)h[y * 12 + 2 * j + 1] << 16);
-                    uint2* o2 = reinterpret_cast<uint2*>(o);
-                    o2[0] = make_uint2(w[0], w[1]);
-                    o2[1] = make_uint2(w[2], w[3]);
-                    o2[2] = make_uint2(w[4], w[5]);
-                } else {
-                    for (int j = 0; j < 12; j++) o[j] = h[y * 12 + j];
-                }
-            } else {
-                float* o = reinterpret_cast<float*>(out) + row;
-                float f[12];
-#pragma unroll
-                for (int j = 0; j < 12; j++) f[j] = __half2float(__ushort_as_half(h[y * 12 + j]));
-                if (aligned) {
-                    float4* o4 = reinterpret_cast<float4*>(o);
-                    o4[0] = make_float4(f[0], f[1], f[2], f[3]);
-                    o4[1] = make_float4(f[4], f[5], f[6], f[7]);
-                    o4[2] = make_float4(f[8], f[9], f[10], f[11]);
-                } else {
-                    for (int j = 0; j < 12; j++) o[j] = f[j];
-                }
+                if (fmt == 0) reinterpret_cast<uint8_t*>(out)[row + 4 * x + 3] = 0;
             }
         }
     }
@@ -322,7 +543,13 @@ static int grid_for(uint32_t n) {
 void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s) {
     if (bw == 0 || bh == 0) return;
     bool aligned = ((uintptr_t)blocks % 16 == 0) && ((uintptr_t)out % 16 == 0) && (pitch % 16 == 0);
-    bc7_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, aligned);
+    if (aligned) {
+        uint32_t g = (bw * bh + kSortCta * kSortItems - 1) / (kSortCta * kSortItems);
+        g = g > 148u * 16u ? 148u * 16u : g;
+        bc7_decode_sorted_kernel<<<g, kSortCta, 0, s>>>(blocks, bw, bh, out, pitch);
+    } else {
+        bc7_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch);
+    }
 }
 
 void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
@@ -332,7 +559,13 @@ void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* o
     // (RGBA16F, rows start at 32-byte multiples) or 16 B (RGBA32F)
     size_t esize = out_format == 0 ? 1 : (out_format == 1 ? 2 : 4);
     bool aligned = ((uintptr_t)blocks % 16 == 0) && ((uintptr_t)out % 16 == 0) && ((pitch * esize) % 16 == 0);
-    bc6h_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, out_format, aligned);
+    if (aligned) {
+        uint32_t g = (bw * bh + kSortCta - 1) / kSortCta;
+        g = g > 148u * 32u ? 148u * 32u : g;
+        bc6h_decode_sorted_kernel<<<g, kSortCta, 0, s>>>(blocks, bw, bh, out, pitch, out_format);
+    } else {
+        bc6h_decode_kernel<<<grid_for(bw * bh), 128, 0, s>>>(blocks, bw, bh, out, pitch, out_format);
+    }
 }
 
 }  // namespace bcn

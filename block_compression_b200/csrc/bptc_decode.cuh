@@ -87,7 +87,7 @@ BCN_DEV uint32_t expand8(uint32_t v) {
 // BPTC index weights (0..64) of 2-, 3- and 4-bit indices, as byte tables.
 template <int IB>
 BCN_DEV uint32_t bptc_weight(uint32_t i) {
-    if (IB == 2) return __byte_perm(0x402B1500u, 0u, i) & 0xFFu;
+    if (IB == 2) return __byte_perm(0x402B1500u, 0u, i | 0x4440u);  // bytes 1-3 from the zero word
     if (IB == 3) return __byte_perm(0x1B120900u, 0x40372E25u, i) & 0xFFu;
     uint32_t lo = __byte_perm(0x0D090400u, 0x1E1A1511u, i & 7u), hi = __byte_perm(0x2F2B2622u, 0x403C3733u, i & 7u);
     return ((i & 8u) ? hi : lo) & 0xFFu;
@@ -154,36 +154,57 @@ BCN_DEV void decode_bc7_mode(const uint32_t d[5], uint32_t out[16]) {
         y = bits64_at(d, IS + T1) & ((1ull << (16 * IB2 - 1)) - 1ull);
         y = insert_zero(y, IB2 - 1);
     }
+    // Per subset: base = e0 * 64 + 32 and delta = e1 - e0 in two 16-bit lanes,
+    // so a texel pair is base + delta * w. Lanes may borrow from each other in
+    // the delta, but the sum is e0 * (64 - w) + e1 * w + 32 exactly (modulo
+    // 2^32), whose lanes never exceed 16 bits.
+    uint32_t brg[NS], drg[NS], bba[NS], dba[NS], da[NS];
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+        brg[j] = erg[2 * j] * 64u + 0x00200020u;
+        drg[j] = erg[2 * j + 1] - erg[2 * j];
+        bba[j] = eba[2 * j] * 64u + 0x00200020u;
+        if constexpr (IB2 > 0) {  // B and A interpolate with different weights
+            dba[j] = (eba[2 * j + 1] & 0xFFFFu) - (eba[2 * j] & 0xFFFFu);
+            da[j] = ((eba[2 * j + 1] >> 16) - (eba[2 * j] >> 16)) << 16;
+        } else {
+            dba[j] = eba[2 * j + 1] - eba[2 * j];
+            da[j] = 0;
+        }
+    }
     // rotation: swap alpha with R (1), G (2) or B (3)
     const uint32_t rot_sel = rot == 1 ? 0x0213u : (rot == 2 ? 0x1230u : (rot == 3 ? 0x2310u : 0x3210u));
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         uint32_t s = NS > 1 ? ((map >> (2 * k)) & 3u) : 0u;
-        uint32_t e0rg = erg[0], e1rg = erg[1], e0ba = eba[0], e1ba = eba[1];
-        if (NS > 1 && s == 1) {
-            e0rg = erg[2];
-            e1rg = erg[3];
-            e0ba = eba[2];
-            e1ba = eba[3];
+        uint32_t b_rg = brg[0], d_rg = drg[0], b_ba = bba[0], d_ba = dba[0], d_a = da[0];
+        if constexpr (NS > 1) {
+            if (s == 1) {
+                b_rg = brg[1];
+                d_rg = drg[1];
+                b_ba = bba[1];
+                d_ba = dba[1];
+            }
         }
-        if (NS > 2 && s == 2) {
-            e0rg = erg[NEP > 4 ? 4 : 0];
-            e1rg = erg[NEP > 5 ? 5 : 1];
-            e0ba = eba[NEP > 4 ? 4 : 0];
-            e1ba = eba[NEP > 5 ? 5 : 1];
+        if constexpr (NS > 2) {
+            if (s == 2) {
+                b_rg = brg[2];
+                d_rg = drg[2];
+                b_ba = bba[2];
+                d_ba = dba[2];
+            }
         }
         uint32_t w1 = bptc_weight<IB>((uint32_t)(x >> (k * IB)) & ((1u << IB) - 1u));
         uint32_t px;
         if constexpr (IB2 > 0) {
             uint32_t w2 = bptc_weight<IB2>((uint32_t)(y >> (k * IB2)) & ((1u << IB2) - 1u));
             uint32_t wc = isb ? w2 : w1, wa = isb ? w1 : w2;
-            uint32_t rg = lerp2(e0rg, e1rg, wc);
-            uint32_t lo = (e0ba & 0xFFFFu) * (64u - wc) + (e1ba & 0xFFFFu) * wc;
-            uint32_t hi = (e0ba >> 16) * (64u - wa) + (e1ba >> 16) * wa;
-            uint32_t ba = (lo + (hi << 16) + 0x00200020u) >> 6;
+            uint32_t rg = (b_rg + d_rg * wc) >> 6;
+            uint32_t ba = (b_ba + d_ba * wc + d_a * wa) >> 6;
             px = __byte_perm(__byte_perm(rg, ba, 0x6420u), 0u, rot_sel);
         } else {
-            px = __byte_perm(lerp2(e0rg, e1rg, w1), lerp2(e0ba, e1ba, w1), 0x6420u);
+            (void)d_a;
+            px = __byte_perm((b_rg + d_rg * w1) >> 6, (b_ba + d_ba * w1) >> 6, 0x6420u);
         }
         out[k] = px;
     }
