@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libbcn_b200.so")
-SOURCES = ["bc15.cu", "bc7_encode.cu", "bc6h_encode.cu", "bc_decode.cu", "capi.cu", "batch.cu", "mips.cu", "refine.cu"]
+SOURCES = ["bc15.cu", "bc7_encode.cu", "bc6h_encode.cu", "bc_decode.cu", "capi.cu", "batch.cu", "mips.cu", "refine.cu",
+           "metrics.cu", "dds.cu"]
 HEADERS = ["bc_common.cuh", "bptc_math.cuh", "bc_kernels.h", "bc7_device.cuh", "bptc_decode.cuh", "bc1_block.cuh",
            "bc_relaxed.cuh"]
 

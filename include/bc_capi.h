@@ -297,6 +297,31 @@ int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, 
                          uint8_t* blocks, size_t blocks_len, uint32_t steps, float lr,
                          uint64_t* stats, float* endpoints_out, void* stream);
 
+/* ---- image-quality metric (the reference's test metric,
+ * tests/metrics.rs:40-114, computed on the GPU) ----------------------------------
+ * Per-channel sums of squared differences between two RGBA8 images a and b
+ * (row pitches in bytes, 4-byte aligned) over the first `channels` channels,
+ * in f64: RGB compared after sRGB -> linear (tests/common/mod.rs:17-24),
+ * alpha as a / 255. sse_out: 4 doubles in device memory (unused channels are
+ * 0). MSE = sse / (width * height); the reference's overall MSE is the mean of
+ * the 4 channel MSEs over `channels`, PSNR = 20 log10(1 / sqrt(MSE)) (0 when
+ * MSE is 0). The partial sums are added in a fixed order, so results do not
+ * vary between runs; they may differ from a sequential sum in the last bits. */
+int bc_image_sse_rgba8_device(const uint8_t* a, size_t pitch_a, const uint8_t* b, size_t pitch_b,
+                              uint32_t width, uint32_t height, uint32_t channels, double* sse_out,
+                              void* stream);
+
+/* ---- DDS container (the reference CLI's output, compressor/src/main.rs:313-353)
+ * bc_dds_header writes the 148-byte header of a DX10-extended DDS file for one
+ * 2D texture: "DDS " + DDS_HEADER + DDS_HEADER_DXT10, straight alpha, the
+ * given mip count (the block data of every level follows the header, largest
+ * first). srgb != 0 selects the _SRGB DXGI formats for BC1/BC2/BC3/BC7, as the
+ * reference CLI does (:343-353); BC4/BC5 are UNORM, BC6H is UF16. */
+#define BC_DDS_HEADER_BYTES 148u
+int bc_dds_header(int variant, uint32_t width, uint32_t height, uint32_t mip_levels, int srgb,
+                  uint8_t* out, size_t out_len);
+uint32_t bc_dds_dxgi_format(int variant, int srgb);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* cudaError_t of the last CUDA failure seen on this thread (0 if none). */
 int bc_last_cuda_error(void);
