@@ -222,14 +222,19 @@ BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const float cb[16], 
     q0 = 0;
     q1 = 0;
     float total = 0.0f;
+    // ep are dequantised values in [0, 255]: (64 - w) * ia + w * ib + 32 =
+    // (64 * ia + 32) + w * (ib - ia) >= 0, so / 64 is >> 6
     int ia = (int)ep[0], ib = (int)ep[1];
+    const int bs = ia * 64 + 32, df = ib - ia;
+    const float den = ep[1] - ep[0] + 0.001f;
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        float proj = (cb[k] - ep[0]) / (ep[1] - ep[0] + 0.001f);
+        float proj = (cb[k] - ep[0]) / den;
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
-        int w0 = unquant_w(bits, q1i - 1), w1 = unquant_w(bits, q1i);
-        float d0 = (float)(((64 - w0) * ia + w0 * ib + 32) / 64);
-        float d1 = (float)(((64 - w1) * ia + w1 * ib + 32) / 64);
+        int w0 = bits == 2 ? bptc_w<2>(q1i - 1) : (bits == 3 ? bptc_w<3>(q1i - 1) : unquant_w(bits, q1i - 1));
+        int w1 = bits == 2 ? bptc_w<2>(q1i) : (bits == 3 ? bptc_w<3>(q1i) : unquant_w(bits, q1i));
+        float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
+        float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
         float err0 = 0.0f, err1 = 0.0f;
         err0 += sqf(d0 - cb[k]);
         err1 += sqf(d1 - cb[k]);

@@ -33,6 +33,14 @@
 #include "bc_kernels.h"
 #include "bptc_math.cuh"
 #include "bc7_device.cuh"
+
+// Minimum resident CTAs per SM requested from the register allocator.
+#ifndef BCN_MODE45_MINB
+#define BCN_MODE45_MINB 5
+#endif
+#ifndef BCN_REFINE_MINB
+#define BCN_REFINE_MINB 4
+#endif
 namespace bcn {
 namespace bc7 {
 
@@ -268,7 +276,7 @@ __global__ void __launch_bounds__(NW * 32) bc7_search_kernel(Work w) {
 // K3: refinement of each block's winning partition + coding (bc7.rs:571-609).
 // One warp per tile.
 template <int MODE, int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_refine_kernel(Work w, uint32_t ntiles) {
+__global__ void __launch_bounds__(NW * 32, BCN_REFINE_MINB) bc7_refine_kernel(Work w, uint32_t ntiles) {
     constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
     __shared__ float px[NW][64][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -297,7 +305,7 @@ __global__ void __launch_bounds__(NW * 32) bc7_refine_kernel(Work w, uint32_t nt
 // launch per index-swap setting. Grid: (tile, rotation group), warp = one
 // rotation for the tile's 32 blocks.
 template <int MODE, int SWAP, bool CH4, int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_mode45_kernel(Work w) {
+__global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Work w) {
     __shared__ float px[64][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;

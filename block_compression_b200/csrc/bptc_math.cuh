@@ -195,40 +195,71 @@ BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
     }
 }
 
-// common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8.
+// BPTC index weight (common.rs:6-21) of a BITS-bit index as a byte-table
+// lookup: the 4/8/16 weights packed in registers and selected with a byte
+// permute.
+template <int BITS>
+BCN_DEV int bptc_w(int i) {
+    if (BITS == 2) return (int)__byte_perm(0x402B1500u, 0u, (uint32_t)i | 0x4440u);
+    if (BITS == 3) return (int)(__byte_perm(0x1B120900u, 0x40372E25u, (uint32_t)i) & 0xFFu);
+    uint32_t lo = __byte_perm(0x0D090400u, 0x1E1A1511u, (uint32_t)i & 7u);
+    uint32_t hi = __byte_perm(0x2F2B2622u, 0x403C3733u, (uint32_t)i & 7u);
+    return (int)(((i & 8) ? hi : lo) & 0xFFu);
+}
+
+template <int PAIRS, class T>
+BCN_DEV T sel_pair(int j, T a, T b, T c) {
+    return PAIRS == 1 ? a : (PAIRS == 2 ? (j == 0 ? a : b) : (j == 0 ? a : (j == 1 ? b : c)));
+}
+
+// common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8, dequantised
+// values in [0, 255]. Everything that depends only on the pair is computed
+// once per pair with the reference's own operations (so the per-pixel values
+// are the same numbers): eb - ea, the sum of its squares, and the decoder's
+// interpolation (64 - w) * ia + w * ib + 32 written as
+// (64 * ia + 32) + w * (ib - ia), which is non-negative, so / 64 is >> 6.
 template <int CH, int BITS, int PAIRS, class B>
 BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
     constexpr int levels = 1 << BITS;
+    float dd[PAIRS][CH], dv[PAIRS];
+    int base[PAIRS][CH], dif[PAIRS][CH];
+#pragma unroll
+    for (int j = 0; j < PAIRS; j++) {
+        float div = 0.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            dd[j][p] = ep[8 * j + 4 + p] - ep[8 * j + p];
+            div += sqf(dd[j][p]);
+            int ia = (int)ep[8 * j + p], ib = (int)ep[8 * j + 4 + p];
+            base[j][p] = ia * 64 + 32;
+            dif[j][p] = ib - ia;
+        }
+        dv[j] = div;
+    }
     float total = 0.0f;
     q0 = 0;
     q1 = 0;
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         int j = PAIRS == 1 ? 0 : (int)((pattern >> (2 * k)) & 3);
-        float ea[CH], eb[CH];
+        float proj = 0.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
-            ea[p] = PAIRS == 1 ? ep[p] : (PAIRS == 2 ? (j == 0 ? ep[p] : ep[8 + p]) : sel3(j, ep[p], ep[8 + p], ep[16 + p]));
-            eb[p] = PAIRS == 1 ? ep[4 + p]
-                               : (PAIRS == 2 ? (j == 0 ? ep[4 + p] : ep[12 + p]) : sel3(j, ep[4 + p], ep[12 + p], ep[20 + p]));
+            float ea = sel_pair<PAIRS>(j, ep[p], ep[8 + (PAIRS > 1 ? p : 0)], ep[16 + (PAIRS > 2 ? p : 0)]);
+            float d = sel_pair<PAIRS>(j, dd[0][p], dd[PAIRS > 1 ? 1 : 0][p], dd[PAIRS > 2 ? 2 : 0][p]);
+            proj += (blk(p, k) - ea) * d;
         }
-        float proj = 0.0f, div = 0.0f;
-#pragma unroll
-        for (int p = 0; p < CH; p++) {
-            float v = blk(p, k);
-            proj += (v - ea[p]) * (eb[p] - ea[p]);
-            div += sqf(eb[p] - ea[p]);
-        }
-        proj /= div;
+        proj /= sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
-        int w0 = unquant_w(BITS, q1i - 1), w1 = unquant_w(BITS, q1i);
+        int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
         float err0 = 0.0f, err1 = 0.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
-            int ia = (int)ea[p], ib = (int)eb[p];
+            int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
+            int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
             float v = blk(p, k);
-            float d0 = (float)(((64 - w0) * ia + w0 * ib + 32) / 64);
-            float d1 = (float)(((64 - w1) * ia + w1 * ib + 32) / 64);
+            float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
+            float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
             err0 += sqf(d0 - v);
             err1 += sqf(d1 - v);
         }
