@@ -482,11 +482,10 @@ def refine_bench(args):
             torch.cuda.synchronize()
             a, b = ev(), ev()
             a.record()
-            for t, w in zip(timgs, work):
-                if per == 16:
-                    refine.refine_bc7(t, w, channels=3, steps=20, lr=0.5, stats=stats)
-                else:
-                    refine.refine_bc1(t, w, steps=20, lr=0.5, stats=stats)
+            if per == 16:
+                refine.refine_bc7_images(list(zip(timgs, work)), channels=3, steps=20, lr=0.5, stats=stats)
+            else:
+                refine.refine_bc1_images(list(zip(timgs, work)), steps=20, lr=0.5, stats=stats)
             b.record()
             torch.cuda.synchronize()
             if i >= args.warmup:

@@ -96,8 +96,9 @@ BCN_DEV uint32_t bptc_weight(uint32_t i) {
 // Two 8-bit channels in 16-bit lanes, interpolated with one weight.
 BCN_DEV uint32_t lerp2(uint32_t e0, uint32_t e1, uint32_t w) { return (e0 * (64u - w) + e1 * w + 0x00200020u) >> 6; }
 
-template <int MODE>
-BCN_DEV void decode_bc7_mode(const uint32_t d[5], uint32_t out[16]) {
+// emit(k, texel) receives pixel k's RGBA8 texel (R in the low byte).
+template <int MODE, class Emit>
+BCN_DEV void decode_bc7_mode(const uint32_t d[5], Emit&& emit) {
     constexpr int NS = (MODE == 0 || MODE == 2) ? 3 : ((MODE == 1 || MODE == 3 || MODE == 7) ? 2 : 1);
     constexpr int NEP = 2 * NS;
     constexpr int PB = MODE == 0 ? 4 : (NS > 1 ? 6 : 0);
@@ -206,26 +207,34 @@ BCN_DEV void decode_bc7_mode(const uint32_t d[5], uint32_t out[16]) {
             (void)d_a;
             px = __byte_perm((b_rg + d_rg * w1) >> 6, (b_ba + d_ba * w1) >> 6, 0x6420u);
         }
-        out[k] = px;
+        emit(k, px);
     }
 }
 
-BCN_DEV void decode_bc7_block(uint64_t lo, uint64_t hi, uint32_t out[16]) {
+// Decodes one BC7 block, handing each texel to emit(k, texel); a reserved
+// mode encoding gives 16 zero texels.
+template <class Emit>
+BCN_DEV void decode_bc7_each(uint64_t lo, uint64_t hi, Emit&& emit) {
     const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
     uint32_t low = d[0] & 0xFFu;
     int mode = low ? __ffs((int)low) - 1 : 8;
     switch (mode) {
-        case 0: decode_bc7_mode<0>(d, out); break;
-        case 1: decode_bc7_mode<1>(d, out); break;
-        case 2: decode_bc7_mode<2>(d, out); break;
-        case 3: decode_bc7_mode<3>(d, out); break;
-        case 4: decode_bc7_mode<4>(d, out); break;
-        case 5: decode_bc7_mode<5>(d, out); break;
-        case 6: decode_bc7_mode<6>(d, out); break;
-        case 7: decode_bc7_mode<7>(d, out); break;
+        case 0: decode_bc7_mode<0>(d, emit); break;
+        case 1: decode_bc7_mode<1>(d, emit); break;
+        case 2: decode_bc7_mode<2>(d, emit); break;
+        case 3: decode_bc7_mode<3>(d, emit); break;
+        case 4: decode_bc7_mode<4>(d, emit); break;
+        case 5: decode_bc7_mode<5>(d, emit); break;
+        case 6: decode_bc7_mode<6>(d, emit); break;
+        case 7: decode_bc7_mode<7>(d, emit); break;
         default:
 #pragma unroll
-            for (int k = 0; k < 16; k++) out[k] = 0u;
+            for (int k = 0; k < 16; k++) emit(k, 0u);
     }
 }
+
+BCN_DEV void decode_bc7_block(uint64_t lo, uint64_t hi, uint32_t out[16]) {
+    decode_bc7_each(lo, hi, [&](int k, uint32_t px) { out[k] = px; });
+}
+
 }  // namespace bcn

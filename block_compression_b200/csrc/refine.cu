@@ -84,10 +84,20 @@ BCN_DEV uint32_t exact_err(const uint32_t dec[16], const uint32_t src[16], uint3
     return err;
 }
 
+// Squared error of one texel over the first `channels` channels: per-byte
+// absolute differences, then the dot product of those bytes with themselves.
+BCN_DEV uint32_t texel_err(uint32_t a, uint32_t b, uint32_t channels) {
+    uint32_t d = __vabsdiffu4(a, b);
+    if (channels == 3) d &= 0x00FFFFFFu;
+    return (uint32_t)__dp4a(d, d, 0u);
+}
+
+// Exact error of a coded block, decoded texel by texel (no texel array).
 BCN_DEV uint32_t bc7_exact_err(uint4 blk, const uint32_t src[16], uint32_t channels) {
-    uint32_t dec[16];
-    decode_bc7_block((uint64_t)blk.x | ((uint64_t)blk.y << 32), (uint64_t)blk.z | ((uint64_t)blk.w << 32), dec);
-    return exact_err(dec, src, channels);
+    uint32_t err = 0;
+    decode_bc7_each((uint64_t)blk.x | ((uint64_t)blk.y << 32), (uint64_t)blk.z | ((uint64_t)blk.w << 32),
+                    [&](int k, uint32_t px) { err += texel_err(px, src[k], channels); });
+    return err;
 }
 
 BCN_DEV uint32_t bc1_exact_err(uint32_t w0, uint32_t w1, const uint32_t src[16]) {
@@ -329,12 +339,30 @@ __global__ void __launch_bounds__(kThreads) bc1_adjoint_kernel(const uint32_t* _
 
 // ---- fused refinement -----------------------------------------------------------
 
-__global__ void __launch_bounds__(kThreads) bc7_endpoint_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
-                                                              bool src_aligned, uint32_t bw, uint32_t bh,
-                                                              uint8_t* __restrict__ blocks, bool blk_aligned,
-                                                              uint32_t channels, uint32_t steps, float lr,
-                                                              unsigned long long* __restrict__ stats,
-                                                              float* __restrict__ theta_out) {
+// One launch refines up to kMaxImages images; grid.y selects the image.
+constexpr int kMaxImages = 16;
+struct RefineImage {
+    const uint8_t* src;
+    size_t stride;
+    uint8_t* blocks;
+    float* theta_out;
+    uint32_t bw, bh;
+    bool src_aligned, blk_aligned;
+};
+struct RefineBatch {
+    RefineImage img[kMaxImages];
+};
+
+__global__ void __launch_bounds__(kThreads) bc7_endpoint_refine_kernel(const __grid_constant__ RefineBatch batch,
+                                                                       uint32_t channels, uint32_t steps, float lr,
+                                                                       unsigned long long* __restrict__ stats) {
+    const RefineImage& im = batch.img[blockIdx.y];
+    const uint8_t* __restrict__ src = im.src;
+    const size_t stride = im.stride;
+    const bool src_aligned = im.src_aligned, blk_aligned = im.blk_aligned;
+    const uint32_t bw = im.bw, bh = im.bh;
+    uint8_t* __restrict__ blocks = im.blocks;
+    float* __restrict__ theta_out = im.theta_out;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < bw * bh;
     uint32_t active = 0, improved = 0, before = 0, after = 0;
@@ -361,6 +389,7 @@ __global__ void __launch_bounds__(kThreads) bc7_endpoint_refine_kernel(const uin
                 float ge[24];
 #pragma unroll
                 for (int j = 0; j < 24; j++) ge[j] = 0.0f;
+#pragma unroll
                 for (int k = 0; k < 16; k++) {
                     float px[4], g[4];
                     relax::bc7_relaxed_px(m, th, k, px);
@@ -394,12 +423,16 @@ __global__ void __launch_bounds__(kThreads) bc7_endpoint_refine_kernel(const uin
     add_stats(stats, active, improved, before, after);
 }
 
-__global__ void __launch_bounds__(kThreads) bc1_endpoint_refine_kernel(const uint8_t* __restrict__ src, size_t stride,
-                                                              bool src_aligned, uint32_t bw, uint32_t bh,
-                                                              uint8_t* __restrict__ blocks, bool blk_aligned,
-                                                              uint32_t steps, float lr,
-                                                              unsigned long long* __restrict__ stats,
-                                                              float* __restrict__ theta_out) {
+__global__ void __launch_bounds__(kThreads) bc1_endpoint_refine_kernel(const __grid_constant__ RefineBatch batch,
+                                                                       uint32_t steps, float lr,
+                                                                       unsigned long long* __restrict__ stats) {
+    const RefineImage& im = batch.img[blockIdx.y];
+    const uint8_t* __restrict__ src = im.src;
+    const size_t stride = im.stride;
+    const bool src_aligned = im.src_aligned, blk_aligned = im.blk_aligned;
+    const uint32_t bw = im.bw, bh = im.bh;
+    uint8_t* __restrict__ blocks = im.blocks;
+    float* __restrict__ theta_out = im.theta_out;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool live = i < bw * bh;
     uint32_t active = 0, improved = 0, before = 0, after = 0;
@@ -560,19 +593,70 @@ extern "C" int bc_bc1_decode_adjoint_device(const uint32_t* meta, const float* g
     return finish_launch();
 }
 
+// Validates and launches the images of one refinement call, kMaxImages per
+// launch. bytes_per_block: 16 (BC7) or 8 (BC1).
+template <class Launch>
+int refine_images(const bc_refine_image* images, uint32_t count, uint32_t bytes_per_block, Launch&& launch) {
+    if (count == 0) return BC_OK;
+    if (!images) return BC_ERR_NULL;
+    for (uint32_t i = 0; i < count; i++) {
+        const bc_refine_image& im = images[i];
+        int st = check_refine_args(im.src, im.src_stride, im.width, im.height, im.blocks, im.blocks_len,
+                                   bytes_per_block, 0, 0.0f);
+        if (st != BC_OK) return st;
+    }
+    for (uint32_t first = 0; first < count; first += kMaxImages) {
+        uint32_t n = count - first < (uint32_t)kMaxImages ? count - first : (uint32_t)kMaxImages;
+        RefineBatch b;
+        uint64_t most = 0;
+        for (uint32_t j = 0; j < n; j++) {
+            const bc_refine_image& im = images[first + j];
+            RefineImage& r = b.img[j];
+            r.src = im.src;
+            r.stride = im.src_stride;
+            r.blocks = im.blocks;
+            r.theta_out = im.endpoints_out;
+            r.bw = im.width / 4;
+            r.bh = im.height / 4;
+            r.src_aligned = aligned_to(im.src, 16) && im.src_stride % 16 == 0;
+            r.blk_aligned = aligned_to(im.blocks, bytes_per_block);
+            uint64_t nb = (uint64_t)r.bw * r.bh;
+            most = nb > most ? nb : most;
+        }
+        if (most == 0) continue;
+        launch(b, dim3(grid_for(most), n));
+        int st = finish_launch();
+        if (st != BC_OK) return st;
+    }
+    return BC_OK;
+}
+
+extern "C" int bc_bc7_refine_images_device(const bc_refine_image* images, uint32_t count, uint32_t channels,
+                                           uint32_t steps, float lr, uint64_t* stats, void* stream) {
+    if (channels != 3 && channels != 4) return BC_ERR_SETTINGS;
+    if (!std::isfinite(lr) || lr < 0.0f || steps > 100000) return BC_ERR_SETTINGS;
+    return refine_images(images, count, 16, [&](const RefineBatch& b, dim3 grid) {
+        bc7_endpoint_refine_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(
+            b, channels, steps, lr, reinterpret_cast<unsigned long long*>(stats));
+    });
+}
+
+extern "C" int bc_bc1_refine_images_device(const bc_refine_image* images, uint32_t count, uint32_t steps, float lr,
+                                           uint64_t* stats, void* stream) {
+    if (!std::isfinite(lr) || lr < 0.0f || steps > 100000) return BC_ERR_SETTINGS;
+    return refine_images(images, count, 8, [&](const RefineBatch& b, dim3 grid) {
+        bc1_endpoint_refine_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(
+            b, steps, lr, reinterpret_cast<unsigned long long*>(stats));
+    });
+}
+
 extern "C" int bc_bc7_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, uint32_t height,
                                     uint8_t* blocks, size_t blocks_len, uint32_t channels, uint32_t steps,
                                     float lr, uint64_t* stats, float* endpoints_out, void* stream) {
     int st = check_refine_args(src, src_stride, width, height, blocks, blocks_len, 16, steps, lr);
     if (st != BC_OK) return st;
-    if (channels != 3 && channels != 4) return BC_ERR_SETTINGS;
-    uint32_t bw = width / 4, bh = height / 4;
-    if ((uint64_t)bw * bh == 0) return BC_OK;
-    bool src_al = aligned_to(src, 16) && src_stride % 16 == 0;
-    bc7_endpoint_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
-        src, src_stride, src_al, bw, bh, blocks, aligned_to(blocks, 16), channels, steps, lr,
-        reinterpret_cast<unsigned long long*>(stats), endpoints_out);
-    return finish_launch();
+    const bc_refine_image im = {src, src_stride, width, height, blocks, blocks_len, endpoints_out};
+    return bc_bc7_refine_images_device(&im, 1, channels, steps, lr, stats, stream);
 }
 
 extern "C" int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, uint32_t height,
@@ -580,11 +664,6 @@ extern "C" int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint3
                                     float* endpoints_out, void* stream) {
     int st = check_refine_args(src, src_stride, width, height, blocks, blocks_len, 8, steps, lr);
     if (st != BC_OK) return st;
-    uint32_t bw = width / 4, bh = height / 4;
-    if ((uint64_t)bw * bh == 0) return BC_OK;
-    bool src_al = aligned_to(src, 16) && src_stride % 16 == 0;
-    bc1_endpoint_refine_kernel<<<grid_for((uint64_t)bw * bh), kThreads, 0, (cudaStream_t)stream>>>(
-        src, src_stride, src_al, bw, bh, blocks, aligned_to(blocks, 8), steps, lr,
-        reinterpret_cast<unsigned long long*>(stats), endpoints_out);
-    return finish_launch();
+    const bc_refine_image im = {src, src_stride, width, height, blocks, blocks_len, endpoints_out};
+    return bc_bc1_refine_images_device(&im, 1, steps, lr, stats, stream);
 }

@@ -17,6 +17,8 @@ All tensors are CUDA tensors; calls run on torch's current stream.
   refine_bc7(src, blocks, ...) / refine_bc1(src, blocks, ...): Adam endpoint
     refinement in place; a block is replaced only if its exact error drops.
 """
+import ctypes
+
 from . import _buffers
 from ._lib import check, lib
 
@@ -153,6 +155,46 @@ def _refine(kind, src, blocks, width, height, stride, steps, lr, channels, want_
         check("bc_bc1_refine_device", lib.bc_bc1_refine_device(*args, steps, float(lr), *tail))
     result = RefineStats(stats.cpu().tolist()) if own_stats else None
     return (result, ep_out) if want_endpoints else result
+
+
+class _Image(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_void_p), ("src_stride", ctypes.c_size_t), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("blocks", ctypes.c_void_p), ("blocks_len", ctypes.c_size_t),
+                ("endpoints_out", ctypes.c_void_p)]
+
+
+def _refine_many(kind, images, steps, lr, channels, stats):
+    """images: list of (src (h, w, 4) CUDA uint8, blocks CUDA uint8)."""
+    torch = _torch()
+    arr = (_Image * len(images))()
+    for e, (src, blocks) in zip(arr, images):
+        _cuda_contig(src, "src")
+        _cuda_contig(blocks, "blocks")
+        e.src, e.src_stride = src.data_ptr(), int(src.shape[1]) * 4
+        e.width, e.height = int(src.shape[1]), int(src.shape[0])
+        e.blocks, e.blocks_len = blocks.data_ptr(), blocks.numel() * blocks.element_size()
+        e.endpoints_out = None
+    own = stats is None
+    if own:
+        dev = images[0][1].device if images else "cuda"
+        stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    if kind == "bc7":
+        check("bc_bc7_refine_images_device", lib.bc_bc7_refine_images_device(
+            ctypes.addressof(arr), len(images), channels, steps, float(lr), stats.data_ptr(), _stream()))
+    else:
+        check("bc_bc1_refine_images_device", lib.bc_bc1_refine_images_device(
+            ctypes.addressof(arr), len(images), steps, float(lr), stats.data_ptr(), _stream()))
+    return RefineStats(stats.cpu().tolist()) if own else None
+
+
+def refine_bc7_images(images, channels=4, steps=20, lr=0.5, stats=None):
+    """refine_bc7 over a list of (src, blocks) pairs in as few launches as
+    possible (16 images per launch)."""
+    return _refine_many("bc7", images, steps, lr, channels, stats)
+
+
+def refine_bc1_images(images, steps=20, lr=0.5, stats=None):
+    return _refine_many("bc1", images, steps, lr, 3, stats)
 
 
 def refine_bc7(src, blocks, channels=4, steps=20, lr=0.5, width=None, height=None, stride=None,

@@ -297,6 +297,22 @@ int bc_bc1_refine_device(const uint8_t* src, size_t src_stride, uint32_t width, 
                          uint8_t* blocks, size_t blocks_len, uint32_t steps, float lr,
                          uint64_t* stats, float* endpoints_out, void* stream);
 
+/* Several images in one call (one launch per 16 images, so small images
+ * still fill the GPU). `images` is a host array describing device buffers;
+ * each entry as the arguments of bc_bc7_refine_device. */
+typedef struct bc_refine_image {
+    const uint8_t* src;     /* RGBA8 source rows (device) */
+    size_t src_stride;      /* bytes per source row */
+    uint32_t width, height; /* multiples of 4 */
+    uint8_t* blocks;        /* encoded blocks (device), refined in place */
+    size_t blocks_len;
+    float* endpoints_out;   /* optional final continuous endpoints (device) */
+} bc_refine_image;
+int bc_bc7_refine_images_device(const bc_refine_image* images, uint32_t count, uint32_t channels,
+                                uint32_t steps, float lr, uint64_t* stats, void* stream);
+int bc_bc1_refine_images_device(const bc_refine_image* images, uint32_t count, uint32_t steps,
+                                float lr, uint64_t* stats, void* stream);
+
 /* ---- image-quality metric (the reference's test metric,
  * tests/metrics.rs:40-114, computed on the GPU) ----------------------------------
  * Per-channel sums of squared differences between two RGBA8 images a and b

@@ -254,3 +254,31 @@ def test_refine_argument_errors(bcn, cuda):
         refine.refine_bc7(src, blocks, width=6, height=8)
     stats = refine.refine_bc7(src, blocks, steps=0)
     assert stats.replaced == 0
+
+
+@pytest.mark.parametrize("kind", ["bc7", "bc1"])
+def test_refine_images_equals_per_image(bcn, cuda, kind):
+    """The multi-image entry point gives the same blocks and totals as one
+    call per image (images of different sizes in one launch)."""
+    import torch
+    from block_compression_b200 import refine
+    sizes = [(64, 64), (32, 96), (128, 40)]
+    v = bcn.CompressionVariant.BC7(BC7Settings.opaque_basic()) if kind == "bc7" else bcn.CompressionVariant.BC1
+    imgs, a, b = [], [], []
+    for i, (h, w) in enumerate(sizes):
+        t = torch.from_numpy(synthetic.config4_texture(11, i, h, w)).cuda()
+        blk = _enc(bcn, torch, v, t, w, h)
+        imgs.append(t)
+        a.append(blk.clone())
+        b.append(blk.clone())
+    tot = [0, 0, 0, 0]
+    for t, blk in zip(imgs, a):
+        st = refine.refine_bc7(t, blk, channels=3) if kind == "bc7" else refine.refine_bc1(t, blk)
+        tot = [x + y for x, y in zip(tot, [st.blocks, st.replaced, st.err_before, st.err_after])]
+    if kind == "bc7":
+        st = refine.refine_bc7_images(list(zip(imgs, b)), channels=3)
+    else:
+        st = refine.refine_bc1_images(list(zip(imgs, b)))
+    assert [st.blocks, st.replaced, st.err_before, st.err_after] == tot
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
