@@ -207,31 +207,6 @@ BCN_DEV int bptc_w(int i) {
     return (int)(((i & 8) ? hi : lo) & 0xFFu);
 }
 
-// Packed pairs of f32 (PTX .f32x2, sm_100): two independent IEEE
-// round-to-nearest operations per instruction, no flush of subnormals.
-typedef unsigned long long F2;
-BCN_DEV F2 f2pack(float a, float b) {
-    F2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-BCN_DEV void f2unpack(F2 v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
-BCN_DEV F2 f2add(F2 a, F2 b) {
-    F2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-BCN_DEV F2 f2sub(F2 a, F2 b) {
-    F2 r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-BCN_DEV F2 f2mul(F2 a, F2 b) {
-    F2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-
 template <int PAIRS, class T>
 BCN_DEV T sel_pair(int j, T a, T b, T c) {
     return PAIRS == 1 ? a : (PAIRS == 2 ? (j == 0 ? a : b) : (j == 0 ? a : (j == 1 ? b : c)));
@@ -270,16 +245,15 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
         float proj = 0.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
-            float ea = sel_pair<PAIRS>(j, ep[p], ep[8 + (PAIRS > 1 ? p : 0)], ep[16 + (PAIRS > 2 ? p : 0)]);
+            // indices stay inside the caller's PAIRS * 8 endpoint array
+            float ea = sel_pair<PAIRS>(j, ep[p], ep[PAIRS > 1 ? 8 + p : p], ep[PAIRS > 2 ? 16 + p : p]);
             float d = sel_pair<PAIRS>(j, dd[0][p], dd[PAIRS > 1 ? 1 : 0][p], dd[PAIRS > 2 ? 2 : 0][p]);
             proj += (blk(p, k) - ea) * d;
         }
         proj /= sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
-        // err0 and err1 accumulate side by side in one f32x2 register pair
-        // (each lane rounds exactly like the scalar operation)
-        F2 err = f2pack(0.0f, 0.0f);
+        float err0 = 0.0f, err1 = 0.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
             int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
@@ -287,11 +261,9 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
             float v = blk(p, k);
             float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
             float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
-            F2 t = f2sub(f2pack(d0, d1), f2pack(v, v));
-            err = f2add(err, f2mul(t, t));
+            err0 += sqf(d0 - v);
+            err1 += sqf(d1 - v);
         }
-        float err0, err1;
-        f2unpack(err, err0, err1);
         float be = err1;
         int bq = q1i;
         if (err0 < err1) {
