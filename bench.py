@@ -116,6 +116,23 @@ def _dist():
     return world, rank, local
 
 
+def max_over_ranks(ms, pg, device):
+    """The largest of every rank's time (each rank passes its own); `pg` is
+    torch.distributed (or None for one process)."""
+    if pg is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mpx_s(world, px_per_rank_step, steps, ms):
+    """Whole-job throughput of a weak-scaling run: every rank encodes
+    px_per_rank_step pixels per step; ms is the max-over-ranks time."""
+    return world * px_per_rank_step * steps / (ms / 1e3) / 1e6
+
+
 def cpu_reference(args, world, rank):
     """Reference arm: the reference's encoder restated in C++ (oracle/), all
     host threads, on a bounded sample of the workload."""
@@ -225,13 +242,9 @@ def gpu_bench(args, world, rank, local):
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
-    total_ms = sum(step_ms)
-    if pg:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), pg, dev)
     px_per_step = 4 * W * H
-    value = world * px_per_step * args.steps / (total_ms / 1e3) / 1e6
+    value = job_mpx_s(world, px_per_step, args.steps, total_ms)
 
     # e2e through the host entry points with pinned host buffers
     pin_img = torch.from_numpy(img_np).pin_memory()
@@ -257,12 +270,8 @@ def gpu_bench(args, world, rank, local):
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
-    if pg:
-        t = torch.tensor([e2e_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * px_per_step * args.steps / (e2e_ms / 1e3) / 1e6
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3), pg, dev)
+    e2e_value = job_mpx_s(world, px_per_step, args.steps, e2e_ms)
     h2d = 3 * img_np.nbytes + nrm_np.nbytes
     d2h = sum(v.blocks_byte_size(W, H) for _, v, _ in jobs)
 
