@@ -173,14 +173,36 @@ BCN_DEV uint4 code_mode01237(int qep[24], uint32_t q0, uint32_t q1, int part_id)
     return make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
 }
 
+// Quantised endpoints of a mode (all < 256) as 24 bytes in 6 words; slots a
+// mode does not code (pairs beyond its count, channel 3 below mode 7) are 0.
+template <int MODE>
+BCN_DEV void pack_qep(uint32_t pk[6], const int qep[24]) {
+    using T = ModeTraits<MODE>;
+#pragma unroll
+    for (int w = 0; w < 6; w++) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int i = 4 * w + b;
+            if (i / 8 < T::pairs && (i & 3) < T::ch) v |= (uint32_t)(qep[i] & 0xFF) << (8 * b);
+        }
+        pk[w] = v;
+    }
+}
+
 // Refinement of a mode's winning partition (bc7.rs:571-609), then coding.
 template <int MODE>
 BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, float best_err, uint32_t iters,
                               float opaque_err, uint4& out) {
     using T = ModeTraits<MODE>;
-    int best_qep[24];
+    // the best quantised endpoints (all < 256) kept as 24 bytes in 6 words
+    uint32_t best_pk[6];
     uint32_t bq0, bq1;
-    eval_part<MODE>(blk, map, part_id, best_qep, bq0, bq1);  // re-creates the winner's state
+    {
+        int q[24];
+        eval_part<MODE>(blk, map, part_id, q, bq0, bq1);  // re-creates the winner's state
+        pack_qep<MODE>(best_pk, q);
+    }
     uint32_t pattern = map[part_id];
     for (uint32_t it = 0; it < iters; it++) {
         float ep[24];
@@ -194,19 +216,28 @@ BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, 
         quant_dequant_part<MODE>(qep, ep);
         float err = block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
         if (err < best_err) {
-#pragma unroll
-            for (int i = 0; i < 24; i++) best_qep[i] = qep[i];
+            pack_qep<MODE>(best_pk, qep);
             bq0 = q0;
             bq1 = q1;
             best_err = err;
         }
     }
     if (MODE != 7) best_err += opaque_err;
+    int best_qep[24];
+#pragma unroll
+    for (int i = 0; i < 24; i++) best_qep[i] = (int)((best_pk[i >> 2] >> (8 * (i & 3))) & 0xFF);
     out = code_mode01237<MODE>(best_qep, bq0, bq1, part_id);
     return best_err;
 }
 
 // ---- mode 4/5 (bc7.rs:239-369, 442-492, 657-733) ---------------------------------
+
+// The rotated-out scalar channel of a block, read from shared memory on use
+// (no register copy of its 16 values).
+struct Chan {
+    const float* p;  // channel row of the block's lane in the tile
+    BCN_DEV float operator[](int k) const { return p[k * NB]; }
+};
 
 BCN_DEV void channel_quant_dequant(int qep[2], float ep[2], int epbits) {
     int elevels = 1 << epbits;
@@ -217,7 +248,8 @@ BCN_DEV void channel_quant_dequant(int qep[2], float ep[2], int epbits) {
     }
 }
 
-BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const float cb[16], int bits, const float ep[2]) {
+template <class C>
+BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const C& cb, int bits, const float ep[2]) {
     int levels = 1 << bits;
     q0 = 0;
     q1 = 0;
@@ -247,7 +279,8 @@ BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const float cb[16], 
     return total;
 }
 
-BCN_DEV void channel_opt_endpoints(float ep[2], const float cb[16], int bits, uint32_t q0, uint32_t q1) {
+template <class C>
+BCN_DEV void channel_opt_endpoints(float ep[2], const C& cb, int bits, uint32_t q0, uint32_t q1) {
     int levels = 1 << bits;
     float lm1 = (float)(levels - 1);
     float atb1 = 0.0f, sum_q = 0.0f, sum_qq = 0.0f, sum = 0.0f;
@@ -358,9 +391,7 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
         err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
-    float chan[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) chan[k] = pxlane[(rot * 16 + k) * NB];
+    const Chan chan{pxlane + rot * 16 * NB};
     float aep[2] = {255.0f, 0.0f};
 #pragma unroll
     for (int k = 0; k < 16; k++) {
