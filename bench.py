@@ -444,14 +444,49 @@ def batched_mips_bench(args):
             batch_ms.append(a.elapsed_time(b))
     same = bool(torch.equal(out_plain, out_batch))
     pm, bm = sum(plain_ms) / len(plain_ms), sum(batch_ms) / len(batch_ms)
+    tune = batch.tune.as_dict()
+    batch.close()
+
+    # the same comparison per variant group: BC7 (compute-bound) and BC1/BC5
+    groups = {}
+    for gname, keep in (("bc7", lambda v: v.id == 6), ("bc1_bc5", lambda v: v.id != 6)):
+        sub = [(lv, v, off) for lv, v, off in tasks if keep(v)]
+        gpx = sum(lv.padded_width * lv.padded_height for lv, _, _ in sub)
+        cg = bcn.GpuBlockCompressor()
+        p_ms = []
+        for i in range(args.warmup + args.steps):
+            for lv, v, off in sub:
+                cg.add_compression_task(v, lv.data, lv.padded_width, lv.padded_height, out_plain, blocks_offset=off)
+            a, b = ev(), ev()
+            a.record()
+            cg.compress()
+            b.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                p_ms.append(a.elapsed_time(b))
+        for lv, v, off in sub:
+            cg.add_compression_task(v, lv.data, lv.padded_width, lv.padded_height, out_batch, blocks_offset=off)
+        gb = cg.create_batch(autotune=True)
+        b_ms = []
+        for i in range(args.warmup + args.steps):
+            a, b = ev(), ev()
+            a.record()
+            gb.launch()
+            b.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                b_ms.append(a.elapsed_time(b))
+        gb.close()
+        gp, gbm = sum(p_ms) / len(p_ms), sum(b_ms) / len(b_ms)
+        groups[gname] = {"tasks": len(sub), "encoded_mpx": gpx / 1e6, "plain_ms": gp, "batched_ms": gbm,
+                         "batched_over_plain": gp / gbm}
     print(json.dumps({
         "workload": "%d RGBA8 textures, sides in {16..4096}, full mip chains, BC1/BC5/BC7 alpha_basic round-robin"
                     % args.textures,
         "tasks": len(tasks), "encoded_mpx": px / 1e6, "plain_ms": pm, "batched_ms": bm,
         "plain_mpx_s": px / pm / 1e3, "batched_mpx_s": px / bm / 1e3, "batched_over_plain": pm / bm,
-        "tune": batch.tune.as_dict(), "autotune_s": tune_s, "outputs_identical": same,
+        "tune": tune, "autotune_s": tune_s, "outputs_identical": same, "by_variant": groups,
     }), flush=True)
-    batch.close()
 
 
 def refine_bench(args):
