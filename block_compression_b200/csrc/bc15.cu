@@ -235,10 +235,10 @@ BCN_DEV void load_rgba8(const uint8_t* __restrict__ src, size_t stride, uint32_t
         }
 #pragma unroll
         for (int x = 0; x < 4; x++) {
-            px.r[y * 4 + x] = (float)(w[x] & 0xFF);
-            px.g[y * 4 + x] = (float)((w[x] >> 8) & 0xFF);
-            px.b[y * 4 + x] = (float)((w[x] >> 16) & 0xFF);
-            px.a[y * 4 + x] = (float)(w[x] >> 24);
+            px.r[y * 4 + x] = byte_to_float(w[x], 0);
+            px.g[y * 4 + x] = byte_to_float(w[x], 1);
+            px.b[y * 4 + x] = byte_to_float(w[x], 2);
+            px.a[y * 4 + x] = byte_to_float(w[x], 3);
         }
     }
 }

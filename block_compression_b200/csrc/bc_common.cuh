@@ -25,6 +25,13 @@ BCN_DEV float clampf_r(float x, float lo, float hi) {
     x = x > hi ? hi : x;
     return x;
 }
+// Byte k of w as a float, without an int->float conversion: the byte is
+// placed in the mantissa of 2^23 (0x4B0000bb) and 2^23 subtracted, which is
+// exact for 0..255.
+BCN_DEV float byte_to_float(uint32_t w, int k) {
+    return __int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)k)) - 8388608.0f;
+}
+
 BCN_DEV int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 BCN_DEV float sqf(float x) { return x * x; }
 
