@@ -44,6 +44,11 @@ namespace bc6h {
 
 using namespace bptc;
 
+// Minimum resident CTAs per SM requested from the register allocator.
+#ifndef BCN_BC6H_MINB
+#define BCN_BC6H_MINB 3
+#endif
+
 constexpr int MAXJ = 10;  // encodes per block (slow settings)
 constexpr int NW = 4;
 
@@ -170,6 +175,8 @@ BCN_DEV uint32_t reverse_bits(uint32_t v, int bits) {
 BCN_DEV void bc6h_pack(uint32_t packed[4], const int* qep, int mode) {
     packed[0] = packed[1] = packed[2] = packed[3] = 0;
     const uint32_t prefix[14] = {0, 1, 2, 6, 10, 14, 18, 22, 26, 30, 3, 7, 11, 15};
+    // prefix[mode] without indexing the table at run time
+    const uint32_t prefix_m = mode < 2 ? (uint32_t)mode : (mode < 10 ? (uint32_t)(4 * mode - 6) : (uint32_t)(4 * mode - 37));
     if (mode <= 8) {
         // Delta-coded two-region modes share the skeleton below; the masks
         // and bit placements differ per mode exactly as in the reference.
@@ -347,7 +354,7 @@ BCN_DEV void bc6h_pack(uint32_t packed[4], const int* qep, int mode) {
             else if (mode == 12) q[c] = (uint32_t)d1 + reverse_bits((uint32_t)(d0 >> 10), 2) * 256;
             else q[c] = (uint32_t)d1 + reverse_bits((uint32_t)(d0 >> 10), 6) * 16;
         }
-        packed[0] = prefix[mode];
+        packed[0] = prefix_m;
         packed[1] = (p[2] << 20) + (p[1] << 10) + p[0];
         packed[2] = (q[2] << 20) + (q[1] << 10) + q[0];
     }
@@ -466,7 +473,7 @@ BCN_DEV Plan make_plan(const BC6HSettingsDev& s) {
     return p;
 }
 
-__global__ void __launch_bounds__(NW * 32) bc6h_encode_kernel(const uint8_t* __restrict__ src, size_t stride,
+__global__ void __launch_bounds__(NW * 32, BCN_BC6H_MINB) bc6h_encode_kernel(const uint8_t* __restrict__ src, size_t stride,
                                                                int source_format, uint32_t bw, uint32_t nblocks,
                                                                uint8_t* __restrict__ dst, BC6HSettingsDev S) {
     __shared__ Smem sm;
@@ -528,17 +535,26 @@ __global__ void __launch_bounds__(NW * 32) bc6h_encode_kernel(const uint8_t* __r
                 su.max_span = span;
             }
         }
-        Job jobs[MAXJ];
+        // each encode's state goes straight to shared memory (a local array
+        // indexed by the running count would live in local memory)
         int n = 0;
+        auto keep = [&](const Job& j) {
+            sm.jmode[n][lane] = j.mode;
+            sm.jepb[n][lane] = j.epb;
+#pragma unroll
+            for (int i = 0; i < 6; i++) sm.jqb[n][i][lane] = j.qb[i];
+            n++;
+        };
         Job st;
         st.mode = 0;
         st.epb = 0;
         for (int i = 0; i < 6; i++) st.qb[i] = 0;
         if (S.slow_mode != 0) {
-            const int modes[10] = {0, 1, 2, 5, 6, 9, 10, 11, 12, 13};
+            // modes 0, 1, 2, 5, 6, 9 (two regions), 10..13 (one region)
+            const uint64_t modes = 0xDCBA965210ull;
             for (int i = 0; i < 10; i++) {
-                test_mode(su, modes[i], 0.0f, st);  // margin 0: always passes
-                jobs[n++] = st;
+                test_mode(su, (int)((modes >> (4 * i)) & 15), 0.0f, st);  // margin 0: always passes
+                keep(st);
             }
         } else {
             if (S.fast_skip_threshold > 0) {
@@ -548,22 +564,17 @@ __global__ void __launch_bounds__(NW * 32) bc6h_encode_kernel(const uint8_t* __r
                 test_mode(su, 5, 1.0f / 1.2f, st);
                 test_mode(su, 0, 1.0f / 1.2f, st);
                 test_mode(su, 2, 1.0f, st);
-                jobs[n++] = st;
+                keep(st);
                 if (S.fast_mode == 0) {
                     test_mode(su, 1, 0.0f, st);
-                    jobs[n++] = st;
+                    keep(st);
                 }
             }
             test_mode(su, 10, 0.0f, st);
             test_mode(su, 11, 1.0f, st);
             test_mode(su, 12, 1.0f, st);
             test_mode(su, 13, 1.0f, st);
-            jobs[n++] = st;
-        }
-        for (int j = 0; j < n; j++) {
-            sm.jmode[j][lane] = jobs[j].mode;
-            sm.jepb[j][lane] = jobs[j].epb;
-            for (int i = 0; i < 6; i++) sm.jqb[j][i][lane] = jobs[j].qb[i];
+            keep(st);
         }
     }
 
