@@ -30,7 +30,7 @@ BCN_DEV uint32_t fast_quant(const Px16& px, int p0, int p1) {
     for (int p = 0; p < 3; p++) dir[p] = c1[p] - c0[p];
     float sq_norm = 0.0f;
     for (int p = 0; p < 3; p++) sq_norm += dir[p] * dir[p];
-    float rsq_norm = 1.0f / sq_norm;
+    float rsq_norm = __frcp_rn(sq_norm);  // the IEEE 1 / x
     for (int p = 0; p < 3; p++) dir[p] *= rsq_norm * 3.0f;
     float bias = 0.5f;
     for (int p = 0; p < 3; p++) bias -= c0[p] * dir[p];
@@ -73,7 +73,7 @@ BCN_DEV void bc1_refine(const Px16& px, int pe[2], uint32_t bits, const float dc
         float cxx = 144.0f - 6.0f * sum_q + sum_qq;  // 16*9 - (2*3)*sum_q + sum_qq
         float cyy = sum_qq;
         float cxy = 3.0f * sum_q - sum_qq;
-        float scale = 3.0f * (1.0f / (cxx * cyy - cxy * cxy));
+        float scale = 3.0f * __frcp_rn(cxx * cyy - cxy * cxy);
         for (int p = 0; p < 3; p++) {
             c0[p] = clampf_r((atb1[p] * cyy - atb2[p] * cxy) * scale, 0.0f, 255.0f);
             c1[p] = clampf_r((atb2[p] * cxx - atb1[p] * cxy) * scale, 0.0f, 255.0f);
@@ -135,7 +135,7 @@ BCN_DEV void bc1_core(const Px16& px, uint32_t& w0, uint32_t& w1) {
             n += ax[0] * ax[0];
             n += ax[1] * ax[1];
             n += ax[2] * ax[2];
-            float rn = 1.0f / sqrtf(n);
+            float rn = __frcp_rn(sqrtf(n));
             a[0] *= rn;
             a[1] *= rn;
             a[2] *= rn;
@@ -160,7 +160,7 @@ BCN_DEV void bc1_core(const Px16& px, uint32_t& w0, uint32_t& w1) {
     norm_sq += a[0] * a[0];
     norm_sq += a[1] * a[1];
     norm_sq += a[2] * a[2];
-    float rnorm_sq = 1.0f / norm_sq;
+    float rnorm_sq = __frcp_rn(norm_sq);
     float c0[3], c1[3];
     for (int p = 0; p < 3; p++) {
         c0[p] = clampf_r(dc[p] + min_dot * rnorm_sq * a[p], 0.0f, 255.0f);

@@ -137,7 +137,7 @@ BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qe
     uint32_t pattern = map[part_id];
 #pragma unroll
     for (int j = 0; j < T::pairs; j++)
-        block_segment<T::ch, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
+        block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
     quant_dequant_part<MODE>(qep, ep);
     return block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
 }
@@ -375,7 +375,7 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
     const int swap = SWAP;
     BlkRot<CH4> cb{pxlane, rot < 3 ? rot : -1};
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    block_segment<3, true>(cb, 0xFFFFu, ep);
+    block_segment<3, true, true>(cb, 0xFFFFu, ep);
     int qep[8];
     constexpr int EPB = MODE == 4 ? 5 : 7;
     quant245<EPB, 8>(qep, ep);
@@ -418,7 +418,7 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
 template <int CH>
 BCN_DEV float mode6(const Blk& blk, uint32_t refine, uint4& out) {
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    block_segment<CH, true>(blk, 0xFFFFu, ep);
+    block_segment<CH, true, true>(blk, 0xFFFFu, ep);
     if (CH == 3) {
         ep[3] = 255.0f;
         ep[7] = 255.0f;

@@ -201,11 +201,11 @@ __global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
         if (nb) stats_masked<4>(blk, 0xFFFFu, full_b);
         for (int item = warp; item < na + nb; item += NW) {
             if (item < na) {
-                float b12 = pca_bound_split<3>(blk, subset_mask_from_map(kPartitionMap[item], 0), full_a);
+                float b12 = pca_bound_split<3, true>(blk, subset_mask_from_map(kPartitionMap[item], 0), full_a);
                 keys[0][item][lane] = item + (int)b12 * 64;
             } else {
                 int part = item - na;
-                float b12 = pca_bound_split<4>(blk, subset_mask_from_map(kPartitionMap[part], 0), full_b);
+                float b12 = pca_bound_split<4, true>(blk, subset_mask_from_map(kPartitionMap[part], 0), full_b);
                 keys[1][part][lane] = part + (int)b12 * 64;
             }
         }

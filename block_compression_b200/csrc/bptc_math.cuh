@@ -57,20 +57,37 @@ BCN_DEV void stats_masked(const B& blk, uint32_t mask, float st[15]) {
     }
 }
 
-// common.rs:334-350 (entries of a 3-channel call outside its 6 stay 0)
-template <int CH>
+// x / n for an integer-valued x in [0, 2^24] and a pixel count n in
+// [1, 16], r = RN(1 / n): q = RN(x * r), then one correction step
+// q + RN(x - q * n) * r with fused multiply-adds (Markstein's correction,
+// IBM J. Res. Develop. 34(1), 1990). Over that whole domain it equals the
+// IEEE quotient x / n bit for bit (checked exhaustively on the CPU for every
+// integer x in [0, 2^24] and every n), at three multiply-adds instead of a
+// division.
+BCN_DEV float div_count(float x, float n, float r) {
+    float q = x * r;
+    return fmaf(fmaf(-q, n, x), r, q);
+}
+
+// common.rs:334-350 (entries of a 3-channel call outside its 6 stay 0).
+// INT: the statistics are sums of 8-bit pixel values and their products
+// (integers below 2^24, BC7), so the divisions by the pixel count use
+// div_count; otherwise IEEE division (BC6H's scaled half-float values).
+template <int CH, bool INT = false>
 BCN_DEV void covar_from_stats(float cv[10], const float st[15]) {
-    cv[0] = st[0] - st[10] * st[10] / st[14];
-    cv[1] = st[1] - st[10] * st[11] / st[14];
-    cv[2] = st[2] - st[10] * st[12] / st[14];
-    cv[4] = st[4] - st[11] * st[11] / st[14];
-    cv[5] = st[5] - st[11] * st[12] / st[14];
-    cv[7] = st[7] - st[12] * st[12] / st[14];
+    const float n = st[14], r = __frcp_rn(n);  // RN(1 / n), the IEEE reciprocal
+    auto dv = [&](float x) { return INT ? div_count(x, n, r) : x / n; };
+    cv[0] = st[0] - dv(st[10] * st[10]);
+    cv[1] = st[1] - dv(st[10] * st[11]);
+    cv[2] = st[2] - dv(st[10] * st[12]);
+    cv[4] = st[4] - dv(st[11] * st[11]);
+    cv[5] = st[5] - dv(st[11] * st[12]);
+    cv[7] = st[7] - dv(st[12] * st[12]);
     if (CH == 4) {
-        cv[3] = st[3] - st[10] * st[13] / st[14];
-        cv[6] = st[6] - st[11] * st[13] / st[14];
-        cv[8] = st[8] - st[12] * st[13] / st[14];
-        cv[9] = st[9] - st[13] * st[13] / st[14];
+        cv[3] = st[3] - dv(st[10] * st[13]);
+        cv[6] = st[6] - dv(st[11] * st[13]);
+        cv[8] = st[8] - dv(st[12] * st[13]);
+        cv[9] = st[9] - dv(st[13] * st[13]);
     } else {
         cv[3] = cv[6] = cv[8] = cv[9] = 0.0f;
     }
@@ -103,7 +120,7 @@ BCN_DEV void compute_axis(float axis[4], const float cv[10]) {
             float n = 0.0f;
 #pragma unroll
             for (int p = 0; p < CH; p++) n += sqf(axis[p]);
-            float rn = 1.0f / sqrtf(n);
+            float rn = __frcp_rn(sqrtf(n));  // the IEEE 1 / x
 #pragma unroll
             for (int p = 0; p < CH; p++) a[p] *= rn;
         }
@@ -138,28 +155,28 @@ BCN_DEV float pca_bound(const float cv[10]) {
 }
 
 // common.rs:396-420
-template <int CH>
+template <int CH, bool INT = false>
 BCN_DEV float pca_bound_split(const Blk& blk, uint32_t mask, const float full[15]) {
     float st[15], cv[10];
     stats_masked<CH>(blk, mask, st);
-    covar_from_stats<CH>(cv, st);
+    covar_from_stats<CH, INT>(cv, st);
     float b = 0.0f;
     b += pca_bound<CH>(cv);
 #pragma unroll
     for (int i = 0; i < 15; i++) st[i] = full[i] - st[i];
-    covar_from_stats<CH>(cv, st);
+    covar_from_stats<CH, INT>(cv, st);
     b += pca_bound<CH>(cv);
     return sqrtf(b) * 256.0f;
 }
 
 // common.rs:483-518 (+ bc7.rs:371-379 clamp when CLAMP)
-template <int CH, bool CLAMP, class B>
+template <int CH, bool CLAMP, bool INT = false, class B>
 BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
     float st[15], cv[10], dc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, axis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     stats_masked<CH>(blk, mask, st);
 #pragma unroll
-    for (int p = 0; p < CH; p++) dc[p] = st[10 + p] / st[14];
-    covar_from_stats<CH>(cv, st);
+    for (int p = 0; p < CH; p++) dc[p] = INT ? div_count(st[10 + p], st[14], __frcp_rn(st[14])) : st[10 + p] / st[14];
+    covar_from_stats<CH, INT>(cv, st);
     const float inv_var = 1.0f / 65536.0f;
 #pragma unroll
     for (int i = 0; i < 10; i++) cv[i] *= inv_var;

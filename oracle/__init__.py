@@ -82,6 +82,8 @@ def lib():
         L.oracle_bc7_refine_block.restype = None
         L.oracle_bc1_refine_block.argtypes = [P, P, U32, ctypes.c_float, P, P]
         L.oracle_bc1_refine_block.restype = None
+        L.oracle_check_div_count.argtypes = []
+        L.oracle_check_div_count.restype = ctypes.c_uint64
         _lib = L
     return _lib
 

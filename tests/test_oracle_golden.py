@@ -84,3 +84,10 @@ def test_round_trip_psnr_sanity(oracle_lib):
         dec = oracle_lib.decompress_rgba8(v, blocks, 128, 128).reshape(img.shape)
         mse = np.mean((dec[..., :3].astype(np.float64) - img[..., :3]) ** 2)
         assert 10 * np.log10(255.0 ** 2 / mse) > floor
+
+
+def test_count_division_shortcut_is_exact(oracle_lib):
+    """The BC7 kernels divide integer pixel statistics by a pixel count with
+    a reciprocal and one fused correction step; over every integer numerator
+    in [0, 2^24] and every count 1..16 that must equal IEEE division."""
+    assert oracle_lib.lib().oracle_check_div_count() == 0
