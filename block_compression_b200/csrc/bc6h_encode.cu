@@ -119,8 +119,8 @@ BCN_DEV void compute_qbounds(const Setup& su, float span, int max_span_idx_or_3,
         if (p == max_span_idx_or_3) s *= 2.0f;
         float middle = (su.bounds[p] + su.bounds[3 + p]) / 2.0f;
         float lo = middle - s / 2.0f, hi = middle + s / 2.0f;
-        qb[p] = clampi((int)(lo / 65535.0f * (float)(levels - 1) + 0.5f), 0, levels - 1);
-        qb[3 + p] = clampi((int)(hi / 65535.0f * (float)(levels - 1) + 0.5f), 0, levels - 1);
+        qb[p] = clampi((int)(div_const<65535>(lo) * (float)(levels - 1) + 0.5f), 0, levels - 1);
+        qb[3 + p] = clampi((int)(div_const<65535>(hi) * (float)(levels - 1) + 0.5f), 0, levels - 1);
     }
 }
 
@@ -156,7 +156,7 @@ BCN_DEV void quant_dequant(int qep[24], float ep[24], int epb, const int qb[6]) 
     for (int i = 0; i < 2 * PAIRS; i++)
 #pragma unroll
         for (int p = 0; p < 3; p++) {
-            int q = clampi((int)(ep[i * 4 + p] / 65535.0f * (float)(levels - 1) + 0.5f), 0, levels - 1);
+            int q = clampi((int)(div_const<65535>(ep[i * 4 + p]) * (float)(levels - 1) + 0.5f), 0, levels - 1);
             q = clampi(q, qb[p], qb[3 + p]);
             qep[i * 4 + p] = q;
             ep[i * 4 + p] = (float)unpack_to_uf16(q, epb);
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_MINB) bc6h_encode_kernel(con
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) sm.px[c * 16 + y * 4 + x][b] = (v[x * 3 + c] / 31.0f) * 64.0f;
+            for (int c = 0; c < 3; c++) sm.px[c * 16 + y * 4 + x][b] = div_const<31>(v[x * 3 + c]) * 64.0f;
     }
     __syncthreads();
     const Blk blk{&sm.px[0][lane]};

@@ -40,7 +40,7 @@ BCN_DEV void quant0367_pair(int* qep, const float* ep) {
         for (int b = 0; b < 2; b++) {
 #pragma unroll
             for (int p = 0; p < QCH; p++) {
-                int v = (int)((ep[i * 4 + p] / 255.0f * (float)levels2 - (float)b) / 2.0f + 0.5f) * 2 + b;
+                int v = (int)((div_const<255>(ep[i * 4 + p]) * (float)levels2 - (float)b) / 2.0f + 0.5f) * 2 + b;
                 qb[b][p] = clampi(v, b, levels2 - 1 + b);
                 eb[b][p] = MODE0 ? (float)unpack_to_byte(qb[b][p], 5) : (float)qb[b][p];
             }
@@ -65,7 +65,7 @@ BCN_DEV void quant1_pair(int* qep, const float* ep) {
 #pragma unroll
         for (int i = 0; i < 8; i++) {
             if ((i & 3) == 3) continue;  // channel 3 is neither coded nor in the error
-            int v = (int)((ep[i] / 255.0f * 127.0f - (float)b) / 2.0f + 0.5f) * 2 + b;
+            int v = (int)((div_const<255>(ep[i]) * 127.0f - (float)b) / 2.0f + 0.5f) * 2 + b;
             qb[b][i] = clampi(v, b, 126 + b);
             eb[b][i] = (float)unpack_to_byte(qb[b][i], 7);
         }
@@ -87,7 +87,7 @@ template <int BITS, int N>
 BCN_DEV void quant245(int* qep, const float* ep) {
     constexpr int levels = 1 << BITS;
 #pragma unroll
-    for (int i = 0; i < N; i++) qep[i] = clampi((int)(ep[i] / 255.0f * (float)(levels - 1) + 0.5f), 0, levels - 1);
+    for (int i = 0; i < N; i++) qep[i] = clampi((int)(div_const<255>(ep[i]) * (float)(levels - 1) + 0.5f), 0, levels - 1);
 }
 
 // ep_quant_dequant for the partitioned modes over PAIRS pairs; channel 3 is
@@ -106,7 +106,7 @@ BCN_DEV void quant_dequant_part(int qep[24], float ep[24]) {
         else {
 #pragma unroll
             for (int i = 0; i < 8; i++)
-                if ((i & 3) != 3) q[i] = clampi((int)(e[i] / 255.0f * 31.0f + 0.5f), 0, 31);
+                if ((i & 3) != 3) q[i] = clampi((int)(div_const<255>(e[i]) * 31.0f + 0.5f), 0, 31);
         }
 #pragma unroll
         for (int i = 0; i < 8; i++) {
@@ -243,7 +243,7 @@ BCN_DEV void channel_quant_dequant(int qep[2], float ep[2], int epbits) {
     int elevels = 1 << epbits;
 #pragma unroll
     for (int i = 0; i < 2; i++) {
-        qep[i] = clampi((int)(ep[i] / 255.0f * (float)(elevels - 1) + 0.5f), 0, elevels - 1);
+        qep[i] = clampi((int)(div_const<255>(ep[i]) * (float)(elevels - 1) + 0.5f), 0, elevels - 1);
         ep[i] = (float)unpack_to_byte(qep[i], epbits);
     }
 }

@@ -32,6 +32,23 @@ BCN_DEV float byte_to_float(uint32_t w, int k) {
     return __int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7540u | (uint32_t)k)) - 8388608.0f;
 }
 
+// x / D for the constant divisors D = 31, 255 and 65535 of the encoders'
+// scale conversions: q = RN(x * RN(1/D)) and one correction step
+// q + RN(x - q * D) * RN(1/D) with fused multiply-adds (Markstein's
+// correction, IBM J. Res. Develop. 34(1), 1990). Equal to the IEEE x / D for
+// every finite float x except x = -0, which gives +0 (checked exhaustively by
+// the oracle test over all 2^32 bit patterns). Every caller scales the
+// quotient and adds a non-zero constant before rounding to an integer, so the
+// sign of a zero quotient does not matter; no caller passes an infinity.
+template <int D>
+BCN_DEV float div_const(float x) {
+    static_assert(D == 31 || D == 255 || D == 65535, "divisor not covered by the exhaustive check");
+    constexpr float d = (float)D;
+    const float r = 1.0f / d;
+    float q = x * r;
+    return fmaf(fmaf(-q, d, x), r, q);
+}
+
 BCN_DEV int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 BCN_DEV float sqf(float x) { return x * x; }
 

@@ -25,3 +25,45 @@ extern "C" uint64_t oracle_check_div_count(void) {
     }
     return bad;
 }
+
+// The same shortcut for the constant divisors of the encoders' scale
+// conversions (bc_common.cuh, div_const): x / d for d in {31, 255, 65535} and
+// every finite float x, in parallel over the 2^32 bit patterns. The only
+// accepted difference is x = -0, where the shortcut gives +0. Returns the
+// number of other mismatches.
+#include <thread>
+#include <vector>
+
+extern "C" uint64_t oracle_check_div_const(float d, int threads) {
+    if (threads < 1) threads = 1;
+    const float r = 1.0f / d;
+    std::vector<uint64_t> bad((size_t)threads, 0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) {
+        pool.emplace_back([&, t] {
+            const uint64_t lo = (1ull << 32) * (uint64_t)t / (uint64_t)threads;
+            const uint64_t hi = (1ull << 32) * (uint64_t)(t + 1) / (uint64_t)threads;
+            uint64_t b = 0;
+            for (uint64_t u = lo; u < hi; u++) {
+                uint32_t bits = (uint32_t)u;
+                float x;
+                std::memcpy(&x, &bits, 4);
+                if (!std::isfinite(x) || bits == 0x80000000u) continue;
+                float q = x * r;
+                float fast = std::fma(std::fma(-q, d, x), r, q);
+                float ieee = x / d;
+                uint32_t a, c;
+                std::memcpy(&a, &fast, 4);
+                std::memcpy(&c, &ieee, 4);
+                b += a != c;
+            }
+            bad[(size_t)t] = b;
+        });
+    }
+    uint64_t total = 0;
+    for (int t = 0; t < threads; t++) {
+        pool[(size_t)t].join();
+        total += bad[(size_t)t];
+    }
+    return total;
+}

@@ -91,3 +91,12 @@ def test_count_division_shortcut_is_exact(oracle_lib):
     a reciprocal and one fused correction step; over every integer numerator
     in [0, 2^24] and every count 1..16 that must equal IEEE division."""
     assert oracle_lib.lib().oracle_check_div_count() == 0
+
+
+@pytest.mark.parametrize("d", [31.0, 255.0, 65535.0])
+def test_constant_division_shortcut_is_exact(oracle_lib, d):
+    """The encoders' scale conversions divide by 31, 255 and 65535 with a
+    reciprocal and one fused correction step; for every finite float
+    numerator (all 2^32 bit patterns, -0 aside) that must equal IEEE
+    division."""
+    assert oracle_lib.lib().oracle_check_div_const(d, os.cpu_count() or 1) == 0
