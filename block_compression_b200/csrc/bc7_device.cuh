@@ -139,7 +139,7 @@ BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qe
     for (int j = 0; j < T::pairs; j++)
         block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
     quant_dequant_part<MODE>(qep, ep);
-    return block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
+    return block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
 }
 
 // bc7.rs:381-440
@@ -214,7 +214,7 @@ BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, 
         int qep[24];
         uint32_t q0, q1;
         quant_dequant_part<MODE>(qep, ep);
-        float err = block_quant<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
+        float err = block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
         if (err < best_err) {
             pack_qep<MODE>(best_pk, qep);
             bq0 = q0;
@@ -382,13 +382,13 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
 #pragma unroll
     for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
     uint32_t q0, q1;
-    float err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
+    float err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
     for (uint32_t it = 0; it < refine; it++) {
         opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
         quant245<EPB, 8>(qep, ep);
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
-        err = block_quant<3, bits, 1>(cb, ep, 0, q0, q1);
+        err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
     const Chan chan{pxlane + rot * 16 * NB};
@@ -428,13 +428,13 @@ BCN_DEV float mode6(const Blk& blk, uint32_t refine, uint4& out) {
 #pragma unroll
     for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
     uint32_t q0, q1;
-    float err = block_quant<CH, 4, 1>(blk, ep, 0, q0, q1);
+    float err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
     for (uint32_t it = 0; it < refine; it++) {
         opt_endpoints<CH, 4>(ep, blk, q0, q1, 0xFFFFu);
         quant0367_pair<7, CH, 4, false>(qep, ep);
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
-        err = block_quant<CH, 4, 1>(blk, ep, 0, q0, q1);
+        err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
     }
     out = code_mode6(qep, q0, q1);
     return err;

@@ -235,10 +235,15 @@ BCN_DEV T sel_pair(int j, T a, T b, T c) {
 // are the same numbers): eb - ea, the sum of its squares, and the decoder's
 // interpolation (64 - w) * ia + w * ib + 32 written as
 // (64 * ia + 32) + w * (ib - ia), which is non-negative, so / 64 is >> 6.
-template <int CH, int BITS, int PAIRS, class B>
+// INT: pixels and endpoints are 8-bit integers (BC7), so the projection is an
+// integer divided by an integer, both at most 4 * 255^2 in magnitude; it is
+// then computed with the divisor's reciprocal and one fused correction step,
+// which equals the IEEE quotient over that whole domain (checked
+// exhaustively by the oracle test). Otherwise IEEE division (BC6H).
+template <int CH, int BITS, int PAIRS, bool INT = false, class B>
 BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
     constexpr int levels = 1 << BITS;
-    float dd[PAIRS][CH], dv[PAIRS];
+    float dd[PAIRS][CH], dv[PAIRS], rdv[PAIRS];
     int base[PAIRS][CH], dif[PAIRS][CH];
 #pragma unroll
     for (int j = 0; j < PAIRS; j++) {
@@ -252,6 +257,7 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
             dif[j][p] = ib - ia;
         }
         dv[j] = div;
+        rdv[j] = INT ? __frcp_rn(div) : 0.0f;
     }
     float total = 0.0f;
     q0 = 0;
@@ -267,7 +273,16 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
             float d = sel_pair<PAIRS>(j, dd[0][p], dd[PAIRS > 1 ? 1 : 0][p], dd[PAIRS > 2 ? 2 : 0][p]);
             proj += (blk(p, k) - ea) * d;
         }
-        proj /= sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
+        {
+            const float y = sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
+            if (INT) {
+                const float r = sel_pair<PAIRS>(j, rdv[0], rdv[PAIRS > 1 ? 1 : 0], rdv[PAIRS > 2 ? 2 : 0]);
+                const float q = proj * r;
+                proj = fmaf(fmaf(-q, y, proj), r, q);
+            } else {
+                proj /= y;
+            }
+        }
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
         float err0 = 0.0f, err1 = 0.0f;

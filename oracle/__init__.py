@@ -86,6 +86,8 @@ def lib():
         L.oracle_check_div_count.restype = ctypes.c_uint64
         L.oracle_check_div_const.argtypes = [ctypes.c_float, ctypes.c_int]
         L.oracle_check_div_const.restype = ctypes.c_uint64
+        L.oracle_check_div_int_pairs.argtypes = [ctypes.c_int]
+        L.oracle_check_div_int_pairs.restype = ctypes.c_uint64
         _lib = L
     return _lib
 

@@ -67,3 +67,39 @@ extern "C" uint64_t oracle_check_div_const(float d, int threads) {
     }
     return total;
 }
+
+// The index fit's projection divides one integer by another (sums of
+// products of 8-bit values: numerator magnitude <= 4 * 255 * 255, divisor in
+// [1, 4 * 255 * 255]); the BC7 kernels do it with the divisor's reciprocal
+// and one fused correction step (bptc_math.cuh, block_quant). Checked here
+// for every positive numerator and divisor in that range; the steps are odd
+// in x, so negative numerators follow, and a zero numerator gives +0 either
+// way (the projection sum starts at +0 and is never -0).
+extern "C" uint64_t oracle_check_div_int_pairs(int threads) {
+    const int M = 4 * 255 * 255;
+    if (threads < 1) threads = 1;
+    std::vector<uint64_t> bad((size_t)threads, 0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) {
+        pool.emplace_back([&, t] {
+            const int lo = 1 + (int)((int64_t)M * t / threads), hi = 1 + (int)((int64_t)M * (t + 1) / threads);
+            uint64_t b = 0;
+            for (int y = lo; y < hi; y++) {
+                const float fy = (float)y, r = 1.0f / fy;
+                for (int x = 1; x <= M; x++) {
+                    const float fx = (float)x;
+                    float q = fx * r;
+                    float fast = std::fma(std::fma(-q, fy, fx), r, q);
+                    b += fast != fx / fy;
+                }
+            }
+            bad[(size_t)t] = b;
+        });
+    }
+    uint64_t total = 0;
+    for (int t = 0; t < threads; t++) {
+        pool[(size_t)t].join();
+        total += bad[(size_t)t];
+    }
+    return total;
+}

@@ -100,3 +100,10 @@ def test_constant_division_shortcut_is_exact(oracle_lib, d):
     numerator (all 2^32 bit patterns, -0 aside) that must equal IEEE
     division."""
     assert oracle_lib.lib().oracle_check_div_const(d, os.cpu_count() or 1) == 0
+
+
+def test_integer_pair_division_shortcut_is_exact(oracle_lib):
+    """The BC7 index fit divides integer sums of 8-bit products by each other
+    with a reciprocal and one fused correction step; for every numerator and
+    divisor in [1, 4 * 255^2] that must equal IEEE division."""
+    assert oracle_lib.lib().oracle_check_div_int_pairs(os.cpu_count() or 1) == 0
