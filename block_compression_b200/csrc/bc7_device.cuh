@@ -258,10 +258,15 @@ BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const C& cb, int bit
     // (64 * ia + 32) + w * (ib - ia) >= 0, so / 64 is >> 6
     int ia = (int)ep[0], ib = (int)ep[1];
     const int bs = ia * 64 + 32, df = ib - ia;
-    const float den = ep[1] - ep[0] + 0.001f;
+    // (cb - ep0) / den: an 8-bit difference over an 8-bit difference plus
+    // 0.001, done with den's reciprocal and one fused correction step, which
+    // gives the IEEE quotient for every such pair (checked exhaustively by
+    // the oracle test)
+    const float den = ep[1] - ep[0] + 0.001f, rden = __frcp_rn(den);
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        float proj = (cb[k] - ep[0]) / den;
+        const float x = cb[k] - ep[0], qx = x * rden;
+        float proj = fmaf(fmaf(-qx, den, x), rden, qx);
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bits == 2 ? bptc_w<2>(q1i - 1) : (bits == 3 ? bptc_w<3>(q1i - 1) : unquant_w(bits, q1i - 1));
         int w1 = bits == 2 ? bptc_w<2>(q1i) : (bits == 3 ? bptc_w<3>(q1i) : unquant_w(bits, q1i));

@@ -88,6 +88,8 @@ def lib():
         L.oracle_check_div_const.restype = ctypes.c_uint64
         L.oracle_check_div_int_pairs.argtypes = [ctypes.c_int]
         L.oracle_check_div_int_pairs.restype = ctypes.c_uint64
+        L.oracle_check_div_channel.argtypes = []
+        L.oracle_check_div_channel.restype = ctypes.c_uint64
         _lib = L
     return _lib
 

@@ -103,3 +103,25 @@ extern "C" uint64_t oracle_check_div_int_pairs(int threads) {
     }
     return total;
 }
+
+// The mode-4/5 scalar-channel fit divides an 8-bit difference x in
+// [-255, 255] by (d + 0.001), d an 8-bit difference in [-255, 255]
+// (channel_opt_quant); the BC7 kernels use the reciprocal and one fused
+// correction step. Every (x, d) pair is checked here.
+extern "C" uint64_t oracle_check_div_channel(void) {
+    uint64_t bad = 0;
+    for (int d = -255; d <= 255; d++) {
+        const float den = (float)d + 0.001f, r = 1.0f / den;
+        for (int xi = -255; xi <= 255; xi++) {
+            const float x = (float)xi;
+            float q = x * r;
+            float fast = std::fma(std::fma(-q, den, x), r, q);
+            float ieee = x / den;
+            uint32_t a, b;
+            std::memcpy(&a, &fast, 4);
+            std::memcpy(&b, &ieee, 4);
+            bad += a != b;
+        }
+    }
+    return bad;
+}

@@ -107,3 +107,10 @@ def test_integer_pair_division_shortcut_is_exact(oracle_lib):
     with a reciprocal and one fused correction step; for every numerator and
     divisor in [1, 4 * 255^2] that must equal IEEE division."""
     assert oracle_lib.lib().oracle_check_div_int_pairs(os.cpu_count() or 1) == 0
+
+
+def test_channel_division_shortcut_is_exact(oracle_lib):
+    """The BC7 mode-4/5 scalar-channel fit divides an 8-bit difference by an
+    8-bit difference plus 0.001 with a reciprocal and one fused correction
+    step; every such pair must give the IEEE quotient."""
+    assert oracle_lib.lib().oracle_check_div_channel() == 0
