@@ -129,15 +129,36 @@ struct ModeTraits {
 };
 
 template <int MODE>
-BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1) {
+BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1,
+                        const float* full = nullptr) {
     using T = ModeTraits<MODE>;
     float ep[24];
 #pragma unroll
     for (int i = 0; i < 24; i++) ep[i] = 0.0f;
     uint32_t pattern = map[part_id];
+    if (T::pairs == 2 && full != nullptr) {
+        // Two subsets, the whole block's statistics given (full[i * NB],
+        // lane-strided like the pixels). Every statistic is a sum of 8-bit
+        // values or of their products, an integer below 2^24 however it is
+        // summed, so the larger subset's statistics are the whole block's
+        // minus the smaller one's, bit for bit. Only the smaller subset is
+        // summed, which also bounds the warp's divergent loop (each lane has
+        // its own partition here) by 8 pixels.
+        const uint32_t m1 = subset_mask_from_map(pattern, 1), m0 = ~m1 & 0xFFFFu;
+        const bool small1 = __popc(m1) <= 8;
+        float ss[15], st[15];
+        stats_masked<T::ch>(blk, small1 ? m1 : m0, ss);
 #pragma unroll
-    for (int j = 0; j < T::pairs; j++)
-        block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
+        for (int i = 0; i < 15; i++) st[i] = small1 ? full[i * NB] - ss[i] : ss[i];
+        block_segment_from_stats<T::ch, true, true>(blk, m0, st, ep);
+#pragma unroll
+        for (int i = 0; i < 15; i++) st[i] = small1 ? ss[i] : full[i * NB] - ss[i];
+        block_segment_from_stats<T::ch, true, true>(blk, m1, st, ep + 8);
+    } else {
+#pragma unroll
+        for (int j = 0; j < T::pairs; j++)
+            block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
+    }
     quant_dequant_part<MODE>(qep, ep);
     return block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
 }

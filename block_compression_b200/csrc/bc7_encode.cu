@@ -36,10 +36,19 @@
 
 // Minimum resident CTAs per SM requested from the register allocator.
 #ifndef BCN_MODE45_MINB
-#define BCN_MODE45_MINB 6
+#define BCN_MODE45_MINB 5
 #endif
 #ifndef BCN_REFINE_MINB
 #define BCN_REFINE_MINB 4
+#endif
+#ifndef BCN_PREP_MINB
+#define BCN_PREP_MINB 4
+#endif
+#ifndef BCN_SEARCH_MINB
+#define BCN_SEARCH_MINB 4
+#endif
+#ifndef BCN_SEARCH13_MINB  // modes 1 and 3 (3 channels, 2 subsets) need fewer registers
+#define BCN_SEARCH13_MINB 5
 #endif
 namespace bcn {
 namespace bc7 {
@@ -185,7 +194,7 @@ BCN_DEV float opaque_err(const Blk& blk, uint32_t channels) {
 // K1: PCA split bounds + ascending top-k partition lists (bc7.rs:622-655,
 // 819-851; common.rs:126-140), and argmin-key initialisation.
 template <int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
+__global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w) {
     __shared__ float px[64][NB];
     __shared__ int keys[2][64][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -194,20 +203,36 @@ __global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
     const Blk blk{&px[0][lane]};
-    const int na = P.bounds_a ? 64 : 0, nb = P.bounds_b ? 64 : 0;
-    if (na + nb > 0) {
-        float full_a[15], full_b[15];
-        if (na) stats_masked<3>(blk, 0xFFFFu, full_a);
-        if (nb) stats_masked<4>(blk, 0xFFFFu, full_b);
-        for (int item = warp; item < na + nb; item += NW) {
-            if (item < na) {
-                float b12 = pca_bound_split<3, true>(blk, subset_mask_from_map(kPartitionMap[item], 0), full_a);
-                keys[0][item][lane] = item + (int)b12 * 64;
-            } else {
-                int part = item - na;
-                float b12 = pca_bound_split<4, true>(blk, subset_mask_from_map(kPartitionMap[part], 0), full_b);
-                keys[1][part][lane] = part + (int)b12 * 64;
-            }
+    if (P.bounds_a && P.bounds_b) {
+        // Both lists: the 4-channel statistics and covariance hold the
+        // 3-channel ones (entries 0-2, 4, 5, 7, 10-12, 14 are the same sums
+        // in the same order), so one pass per partition feeds both bounds.
+        float full[15];
+        stats_masked<4>(blk, 0xFFFFu, full);
+        for (int part = warp; part < 64; part += NW) {
+            float st[15], cv[10];
+            stats_masked<4>(blk, subset_mask_from_map(kPartitionMap[part], 0), st);
+            covar_from_stats<4, true>(cv, st);
+            float ba = 0.0f, bb = 0.0f;
+            ba += pca_bound<3>(cv);
+            bb += pca_bound<4>(cv);
+#pragma unroll
+            for (int i = 0; i < 15; i++) st[i] = full[i] - st[i];
+            covar_from_stats<4, true>(cv, st);
+            ba += pca_bound<3>(cv);
+            bb += pca_bound<4>(cv);
+            keys[0][part][lane] = part + (int)(sqrtf(ba) * 256.0f) * 64;
+            keys[1][part][lane] = part + (int)(sqrtf(bb) * 256.0f) * 64;
+        }
+    } else if (P.bounds_a || P.bounds_b) {
+        const int set = P.bounds_a ? 0 : 1;
+        float full[15];
+        if (set == 0) stats_masked<3>(blk, 0xFFFFu, full);
+        else stats_masked<4>(blk, 0xFFFFu, full);
+        for (int part = warp; part < 64; part += NW) {
+            uint32_t mask = subset_mask_from_map(kPartitionMap[part], 0);
+            float b12 = set == 0 ? pca_bound_split<3, true>(blk, mask, full) : pca_bound_split<4, true>(blk, mask, full);
+            keys[set][part][lane] = part + (int)b12 * 64;
         }
     }
     __syncthreads();
@@ -217,14 +242,11 @@ __global__ void __launch_bounds__(NW * 32) bc7_prep_kernel(Work w) {
         int K = set == 0 ? P.k_a : P.k_b;
         if (K == 0 || warp != set) continue;
         for (int k = 0; k < K; k++) {
-            int best = INT_MAX, bi = 0;
-            for (int q = 0; q < 64; q++) {
-                int v = keys[set][q][lane];
-                if (v < best) {
-                    best = v;
-                    bi = q;
-                }
-            }
+            // the low 6 bits of a key are its partition
+            int best = INT_MAX;
+#pragma unroll 16
+            for (int q = 0; q < 64; q++) best = min(best, keys[set][q][lane]);
+            const int bi = best & 63;
             keys[set][bi][lane] = INT_MAX;
             w.lists[(size_t)(set == 0 ? k : P.k_a + k) * w.npad + gi] = (uint8_t)bi;
         }
@@ -246,22 +268,31 @@ BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
 // patterns order like the values, and the low word breaks ties toward the
 // earlier candidate, exactly the reference's strict "<" scan.
 template <int MODE, int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_search_kernel(Work w) {
+__global__ void __launch_bounds__(NW * 32, (MODE == 1 || MODE == 3 ? BCN_SEARCH13_MINB : BCN_SEARCH_MINB) * 8 / NW)
+    bc7_search_kernel(Work w) {
     constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
+    constexpr bool two = ModeTraits<MODE>::pairs == 2;
     __shared__ float px[64][NB];
+    __shared__ float full[two ? 15 : 1][NB];
     __shared__ unsigned long long best[NW][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
+    const Blk blk{&px[0][lane]};
+    if (two) {
+        // the whole block's statistics, one entry per warp at a time
+        for (int e = warp; e < 15; e += NW) full[e][lane] = stat_entry<ModeTraits<MODE>::ch>(blk, e);
+        __syncthreads();
+    }
     const int c = blockIdx.y * NW + warp;
     unsigned long long key = ~0ull;
     if (c < P.count[mi] && tile_loc(w, tile).valid(lane)) {
-        const Blk blk{&px[0][lane]};
         int qep[24];
         uint32_t q0, q1;
-        float err = eval_part<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1);
+        float err = eval_part<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1,
+                                    two ? &full[0][lane] : nullptr);
         if (err == err) key = ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c;
     }
     best[warp][lane] = key;

@@ -93,11 +93,19 @@ __constant__ __device__ const uint8_t kAnchors[128] = {BCN_ANCHOR_VALUES};
 // reference's packed mask table (src/encode/common.rs:49-83) for subsets 0
 // and 1; for subset 2 the reference returns `!mask0 & !mask1` whose low 16
 // bits are the same set (only the low 16 bits are ever consumed).
-BCN_DEV uint32_t subset_mask_from_map(uint32_t map, uint32_t subset) {
-    uint32_t m = 0;
-#pragma unroll
-    for (int k = 0; k < 16; k++) m |= (((map >> (2 * k)) & 3u) == subset ? 1u : 0u) << k;
-    return m;
+//
+// Bit-parallel form: a 2-bit field equals `subset` exactly when both bits of
+// ~(map ^ subset replicated into every field) are set; the 16 field flags
+// (bits 0, 2, ..., 30) are then gathered into bits 0..15 by the usual
+// halving compress (checked against the per-field definition for every
+// field value, position and subset, and on random maps, by the CPU tests).
+__host__ __device__ __forceinline__ uint32_t subset_mask_from_map(uint32_t map, uint32_t subset) {
+    uint32_t x = ~(map ^ (subset * 0x55555555u));
+    x &= (x >> 1) & 0x55555555u;
+    x = (x | (x >> 1)) & 0x33333333u;
+    x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+    x = (x | (x >> 4)) & 0x00FF00FFu;
+    return (x | (x >> 8)) & 0x0000FFFFu;
 }
 
 // Reference semantics of get_pattern_mask(part_id, j) for the bits the

@@ -169,11 +169,32 @@ BCN_DEV float pca_bound_split(const Blk& blk, uint32_t mask, const float full[15
     return sqrtf(b) * 256.0f;
 }
 
-// common.rs:483-518 (+ bc7.rs:371-379 clamp when CLAMP)
+// Entry e of stats_masked<CH>(blk, 0xFFFF, st) alone: 0-9 the channel
+// products (r*r, r*g, r*b, r*a, g*g, g*b, g*a, b*b, b*a, a*a), 10-13 the
+// channel sums, 14 the pixel count; entries of alpha stay 0 when CH = 3.
+// Summed over all 16 pixels in order, the same as stats_masked.
+template <int CH, class B>
+BCN_DEV float stat_entry(const B& blk, int e) {
+    if (e == 14) return 16.0f;
+    const int ca = e < 4 ? 0 : (e < 7 ? 1 : (e < 9 ? 2 : (e == 9 ? 3 : e - 10)));
+    const int cb = e < 4 ? e : (e < 7 ? e - 3 : (e < 9 ? e - 5 : 3));
+    if (CH == 3 && (ca == 3 || (e < 10 && cb == 3))) return 0.0f;
+    float acc = 0.0f;
+    if (e >= 10) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += blk(ca, k);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += blk(ca, k) * blk(cb, k);
+    }
+    return acc;
+}
+
+// common.rs:483-518 (+ bc7.rs:371-379 clamp when CLAMP), from the subset's
+// statistics st as stats_masked<CH> gives them (st is consumed).
 template <int CH, bool CLAMP, bool INT = false, class B>
-BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
-    float st[15], cv[10], dc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, axis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    stats_masked<CH>(blk, mask, st);
+BCN_DEV void block_segment_from_stats(const B& blk, uint32_t mask, float st[15], float ep[8]) {
+    float cv[10], dc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, axis[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int p = 0; p < CH; p++) dc[p] = INT ? div_count(st[10 + p], st[14], __frcp_rn(st[14])) : st[10 + p] / st[14];
     covar_from_stats<CH, INT>(cv, st);
@@ -210,6 +231,14 @@ BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
         ep[p] = a;
         ep[4 + p] = b;
     }
+}
+
+// common.rs:483-518 with the statistics of the subset's pixels.
+template <int CH, bool CLAMP, bool INT = false, class B>
+BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
+    float st[15];
+    stats_masked<CH>(blk, mask, st);
+    block_segment_from_stats<CH, CLAMP, INT>(blk, mask, st, ep);
 }
 
 // BPTC index weight (common.rs:6-21) of a BITS-bit index as a byte-table
