@@ -128,7 +128,8 @@ struct ModeTraits {
     static constexpr int ch = MODE == 7 ? 4 : 3;
 };
 
-template <int MODE>
+// UNIFORM: every lane of the warp evaluates the same partition.
+template <int MODE, bool UNIFORM = false>
 BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1,
                         const float* full = nullptr) {
     using T = ModeTraits<MODE>;
@@ -160,6 +161,7 @@ BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qe
             block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
     }
     quant_dequant_part<MODE>(qep, ep);
+    if (UNIFORM) return block_quant_by_subset<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
     return block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
 }
 

@@ -44,11 +44,11 @@
 #ifndef BCN_PREP_MINB
 #define BCN_PREP_MINB 4
 #endif
-#ifndef BCN_SEARCH_MINB
-#define BCN_SEARCH_MINB 4
+#ifndef BCN_SEARCH_MINB  // search of modes 0-3
+#define BCN_SEARCH_MINB 5
 #endif
-#ifndef BCN_SEARCH13_MINB  // modes 1 and 3 (3 channels, 2 subsets) need fewer registers
-#define BCN_SEARCH13_MINB 5
+#ifndef BCN_SEARCH7_MINB  // mode 7 (4 channels) needs more registers
+#define BCN_SEARCH7_MINB 4
 #endif
 namespace bcn {
 namespace bc7 {
@@ -268,7 +268,7 @@ BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
 // patterns order like the values, and the low word breaks ties toward the
 // earlier candidate, exactly the reference's strict "<" scan.
 template <int MODE, int NW>
-__global__ void __launch_bounds__(NW * 32, (MODE == 1 || MODE == 3 ? BCN_SEARCH13_MINB : BCN_SEARCH_MINB) * 8 / NW)
+__global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_SEARCH_MINB) * 8 / NW)
     bc7_search_kernel(Work w) {
     constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
     constexpr bool two = ModeTraits<MODE>::pairs == 2;
@@ -291,7 +291,8 @@ __global__ void __launch_bounds__(NW * 32, (MODE == 1 || MODE == 3 ? BCN_SEARCH1
     if (c < P.count[mi] && tile_loc(w, tile).valid(lane)) {
         int qep[24];
         uint32_t q0, q1;
-        float err = eval_part<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1,
+        // modes 0 and 2 search partition c for every block of the tile
+        float err = eval_part<MODE, (mi <= 1)>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1,
                                     two ? &full[0][lane] : nullptr);
         if (err == err) key = ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c;
     }

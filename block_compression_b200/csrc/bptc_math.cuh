@@ -338,6 +338,64 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
     return total;
 }
 
+// block_quant<CH, BITS, PAIRS, true> walking each subset's pixels in turn,
+// with that pair's values in registers instead of selected per pixel. The
+// per-pixel arithmetic is the same; the pixel errors are integers (squared
+// differences of bytes, at most 16 * 4 * 255^2 in total, below 2^24), so
+// their float sum is exact in any order and equals the pixel-order sum.
+// Meant for a pattern shared by the whole warp (no divergent loops).
+template <int CH, int BITS, int PAIRS, class B>
+BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
+    constexpr int levels = 1 << BITS;
+    float total = 0.0f;
+    q0 = 0;
+    q1 = 0;
+#pragma unroll
+    for (int j = 0; j < PAIRS; j++) {
+        float dd[CH], div = 0.0f;
+        int base[CH], dif[CH];
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            dd[p] = ep[8 * j + 4 + p] - ep[8 * j + p];
+            div += sqf(dd[p]);
+            int ia = (int)ep[8 * j + p], ib = (int)ep[8 * j + 4 + p];
+            base[p] = ia * 64 + 32;
+            dif[p] = ib - ia;
+        }
+        const float rdv = __frcp_rn(div);
+        const uint32_t mask = PAIRS == 1 ? 0xFFFFu : subset_mask_from_map(pattern, j);
+        for (uint32_t m = mask; m; m &= m - 1) {
+            const int k = __ffs(m) - 1;
+            float proj = 0.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) proj += (blk(p, k) - ep[8 * j + p]) * dd[p];
+            const float q = proj * rdv;
+            proj = fmaf(fmaf(-q, div, proj), rdv, q);
+            int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
+            int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
+            float err0 = 0.0f, err1 = 0.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                float v = blk(p, k);
+                float d0 = (float)((uint32_t)(base[p] + w0 * dif[p]) >> 6);
+                float d1 = (float)((uint32_t)(base[p] + w1 * dif[p]) >> 6);
+                err0 += sqf(d0 - v);
+                err1 += sqf(d1 - v);
+            }
+            float be = err1;
+            uint32_t bq = (uint32_t)q1i;
+            if (err0 < err1) {
+                be = err0;
+                bq = (uint32_t)(q1i - 1);
+            }
+            if (k < 8) q0 |= bq << (4 * k);
+            else q1 |= bq << (4 * (k - 8));
+            total += be;
+        }
+    }
+    return total;
+}
+
 // common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH).
 template <int CH, int BITS, class B>
 BCN_DEV void opt_endpoints(float* ep, const B& blk, uint32_t q0, uint32_t q1, uint32_t mask) {
