@@ -18,9 +18,13 @@ template <bool CH4>
 struct BlkRot {
     const float* p;
     int rot;
+    // volatile reads: every use is a shared-memory load, so the compiler
+    // keeps no register copy of the block across the refinement loops
+    // (which cost this long kernel spills)
     BCN_DEV float operator()(int c, int k) const {
-        if (c == rot) return CH4 ? p[(48 + k) * NB] : 255.0f;
-        return p[(c * 16 + k) * NB];
+        const volatile float* q = p;
+        if (c == rot) return CH4 ? q[(48 + k) * NB] : 255.0f;
+        return q[(c * 16 + k) * NB];
     }
 };
 
@@ -129,8 +133,8 @@ struct ModeTraits {
 };
 
 // UNIFORM: every lane of the warp evaluates the same partition.
-template <int MODE, bool UNIFORM = false>
-BCN_DEV float eval_part(const Blk& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1,
+template <int MODE, bool UNIFORM = false, class B>
+BCN_DEV float eval_part(const B& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1,
                         const float* full = nullptr) {
     using T = ModeTraits<MODE>;
     float ep[24];
@@ -214,8 +218,8 @@ BCN_DEV void pack_qep(uint32_t pk[6], const int qep[24]) {
 }
 
 // Refinement of a mode's winning partition (bc7.rs:571-609), then coding.
-template <int MODE>
-BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, float best_err, uint32_t iters,
+template <int MODE, class B>
+BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, float best_err, uint32_t iters,
                               float opaque_err, uint4& out) {
     using T = ModeTraits<MODE>;
     // the best quantised endpoints (all < 256) kept as 24 bytes in 6 words
@@ -259,7 +263,7 @@ BCN_DEV float refine_and_code(const Blk& blk, const uint32_t* map, int part_id, 
 // (no register copy of its 16 values).
 struct Chan {
     const float* p;  // channel row of the block's lane in the tile
-    BCN_DEV float operator[](int k) const { return p[k * NB]; }
+    BCN_DEV float operator[](int k) const { return ((const volatile float*)p)[k * NB]; }
 };
 
 BCN_DEV void channel_quant_dequant(int qep[2], float ep[2], int epbits) {
@@ -404,19 +408,21 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
     BlkRot<CH4> cb{pxlane, rot < 3 ? rot : -1};
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     block_segment<3, true, true>(cb, 0xFFFFu, ep);
+    // quantise + index fit, then `refine` times: endpoint fit, quantise +
+    // index fit (one copy of each step in the code: the kernel is
+    // instruction-cache bound)
     int qep[8];
     constexpr int EPB = MODE == 4 ? 5 : 7;
-    quant245<EPB, 8>(qep, ep);
-#pragma unroll
-    for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
     uint32_t q0, q1;
-    float err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
-    for (uint32_t it = 0; it < refine; it++) {
-        opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
+    float err;
+#pragma unroll 1
+    for (uint32_t it = 0;; it++) {
         quant245<EPB, 8>(qep, ep);
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
         err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
+        if (it == refine) break;
+        opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
     const Chan chan{pxlane + rot * 16 * NB};
@@ -428,12 +434,13 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
     }
     int aqep[2];
     uint32_t a0, a1;
-    channel_quant_dequant(aqep, aep, aepbits);
-    float aerr = channel_opt_quant(a0, a1, chan, abits, aep);
-    for (uint32_t it = 0; it < refine_channel; it++) {
-        channel_opt_endpoints(aep, chan, abits, a0, a1);
+    float aerr;
+#pragma unroll 1
+    for (uint32_t it = 0;; it++) {
         channel_quant_dequant(aqep, aep, aepbits);
         aerr = channel_opt_quant(a0, a1, chan, abits, aep);
+        if (it == refine_channel) break;
+        channel_opt_endpoints(aep, chan, abits, a0, a1);
     }
     err += aerr;
 
@@ -443,8 +450,8 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
 
 // ---- mode 6 (bc7.rs:494-515, 762-817) -------------------------------------------
 
-template <int CH>
-BCN_DEV float mode6(const Blk& blk, uint32_t refine, uint4& out) {
+template <int CH, class B>
+BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     block_segment<CH, true, true>(blk, 0xFFFFu, ep);
     if (CH == 3) {

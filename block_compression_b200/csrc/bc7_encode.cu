@@ -183,7 +183,8 @@ BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, 
     }
 }
 
-BCN_DEV float opaque_err(const Blk& blk, uint32_t channels) {
+template <class B>
+BCN_DEV float opaque_err(const B& blk, uint32_t channels) {
     // compute_opaque_err (bc7.rs:869-879)
     float e = 0.0f;
     if (channels != 3)
