@@ -224,30 +224,35 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
     using T = ModeTraits<MODE>;
     // the best quantised endpoints (all < 256) kept as 24 bytes in 6 words
     uint32_t best_pk[6];
-    uint32_t bq0, bq1;
-    {
-        int q[24];
-        eval_part<MODE>(blk, map, part_id, q, bq0, bq1);  // re-creates the winner's state
-        pack_qep<MODE>(best_pk, q);
-    }
-    uint32_t pattern = map[part_id];
-    for (uint32_t it = 0; it < iters; it++) {
-        float ep[24];
+    uint32_t bq0 = 0, bq1 = 0;
+    const uint32_t pattern = map[part_id];
+    float ep[24];
+#pragma unroll
+    for (int i = 0; i < 24; i++) ep[i] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < T::pairs; j++)
+        block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
+    // Pass 0 re-creates the winner's state (its error is best_err already);
+    // passes 1..iters fit the endpoints to the best indices and keep a
+    // strictly better result. One copy of the quantise + index-fit code.
+#pragma unroll 1
+    for (uint32_t it = 0;; it++) {
+        int qep[24];
+        uint32_t q0, q1;
+        quant_dequant_part<MODE>(qep, ep);
+        float err = block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
+        if (it == 0 || err < best_err) {
+            pack_qep<MODE>(best_pk, qep);
+            bq0 = q0;
+            bq1 = q1;
+            if (it != 0) best_err = err;
+        }
+        if (it == iters) break;
 #pragma unroll
         for (int i = 0; i < 24; i++) ep[i] = 0.0f;
 #pragma unroll
         for (int j = 0; j < T::pairs; j++)
             opt_endpoints<T::ch, T::bits>(ep + 8 * j, blk, bq0, bq1, subset_mask_from_map(pattern, j));
-        int qep[24];
-        uint32_t q0, q1;
-        quant_dequant_part<MODE>(qep, ep);
-        float err = block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
-        if (err < best_err) {
-            pack_qep<MODE>(best_pk, qep);
-            bq0 = q0;
-            bq1 = q1;
-            best_err = err;
-        }
     }
     if (MODE != 7) best_err += opaque_err;
     int best_qep[24];
@@ -280,7 +285,7 @@ BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const C& cb, int bit
     int levels = 1 << bits;
     q0 = 0;
     q1 = 0;
-    float total = 0.0f;
+    int total = 0;  // integer pixel errors (pixel_err2), exact
     // ep are dequantised values in [0, 255]: (64 - w) * ia + w * ib + 32 =
     // (64 * ia + 32) + w * (ib - ia) >= 0, so / 64 is >> 6
     int ia = (int)ep[0], ib = (int)ep[1];
@@ -297,18 +302,15 @@ BCN_DEV float channel_opt_quant(uint32_t& q0, uint32_t& q1, const C& cb, int bit
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bits == 2 ? bptc_w<2>(q1i - 1) : (bits == 3 ? bptc_w<3>(q1i - 1) : unquant_w(bits, q1i - 1));
         int w1 = bits == 2 ? bptc_w<2>(q1i) : (bits == 3 ? bptc_w<3>(q1i) : unquant_w(bits, q1i));
-        float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
-        float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
-        float err0 = 0.0f, err1 = 0.0f;
-        err0 += sqf(d0 - cb[k]);
-        err1 += sqf(d1 - cb[k]);
-        float be = err0 < err1 ? err0 : err1;
+        int err0 = 0, err1 = 0;
+        pixel_err2(bs, df, cb[k], w0, w1, err0, err1);
+        int be = err0 < err1 ? err0 : err1;
         int bq = err0 < err1 ? q1i - 1 : q1i;
         if (k < 8) q0 |= (uint32_t)bq << (4 * k);
         else q1 |= (uint32_t)bq << (4 * (k - 8));
         total += be;
     }
-    return total;
+    return (float)total;
 }
 
 template <class C>
@@ -458,18 +460,19 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
         ep[3] = 255.0f;
         ep[7] = 255.0f;
     }
+    // quantise + index fit, then `refine` times: endpoint fit, quantise +
+    // index fit (one copy of each step in the code)
     int qep[8];
-    quant0367_pair<7, CH, 4, false>(qep, ep);
-#pragma unroll
-    for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
     uint32_t q0, q1;
-    float err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
-    for (uint32_t it = 0; it < refine; it++) {
-        opt_endpoints<CH, 4>(ep, blk, q0, q1, 0xFFFFu);
+    float err;
+#pragma unroll 1
+    for (uint32_t it = 0;; it++) {
         quant0367_pair<7, CH, 4, false>(qep, ep);
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
         err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
+        if (it == refine) break;
+        opt_endpoints<CH, 4>(ep, blk, q0, q1, 0xFFFFu);
     }
     out = code_mode6(qep, q0, q1);
     return err;

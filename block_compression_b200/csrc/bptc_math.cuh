@@ -258,6 +258,21 @@ BCN_DEV T sel_pair(int j, T a, T b, T c) {
     return PAIRS == 1 ? a : (PAIRS == 2 ? (j == 0 ? a : b) : (j == 0 ? a : (j == 1 ? b : c)));
 }
 
+// Squared errors of one channel of a pixel against two index weights, in
+// integers: the decoded value is d = (bs + w * df) >> 6 (bs = 64 * e0 + 32,
+// df = e1 - e0, both endpoints bytes) and v is the pixel's byte (an exact
+// integer in a float). Since 64 * v is a multiple of 64,
+// d - v = ((bs - 64 * v) + w * df) >> 6 with an arithmetic shift. Every
+// value involved is an integer well inside 2^24, so the float computation
+// (d - v)^2 summed over the channels -- all exact -- gives the same numbers;
+// the comparisons and totals built from them are unchanged.
+BCN_DEV void pixel_err2(int bs, int df, float v, int w0, int w1, int& err0, int& err1) {
+    const int bsv = bs - ((int)v << 6);
+    const int a0 = (bsv + w0 * df) >> 6, a1 = (bsv + w1 * df) >> 6;
+    err0 += a0 * a0;
+    err1 += a1 * a1;
+}
+
 // common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8, dequantised
 // values in [0, 255]. Everything that depends only on the pair is computed
 // once per pair with the reference's own operations (so the per-pixel values
@@ -289,6 +304,7 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
         rdv[j] = INT ? __frcp_rn(div) : 0.0f;
     }
     float total = 0.0f;
+    int itotal = 0;
     q0 = 0;
     q1 = 0;
 #pragma unroll
@@ -314,28 +330,45 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
         }
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
-        float err0 = 0.0f, err1 = 0.0f;
-#pragma unroll
-        for (int p = 0; p < CH; p++) {
-            int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
-            int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
-            float v = blk(p, k);
-            float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
-            float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
-            err0 += sqf(d0 - v);
-            err1 += sqf(d1 - v);
-        }
-        float be = err1;
         int bq = q1i;
-        if (err0 < err1) {
-            be = err0;
-            bq = q1i - 1;
+        if (INT) {
+            // integer pixel errors, see pixel_err2
+            int err0 = 0, err1 = 0;
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
+                int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
+                pixel_err2(bs, df, blk(p, k), w0, w1, err0, err1);
+            }
+            int be = err1;
+            if (err0 < err1) {
+                be = err0;
+                bq = q1i - 1;
+            }
+            itotal += be;
+        } else {
+            float err0 = 0.0f, err1 = 0.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
+                int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
+                float v = blk(p, k);
+                float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
+                float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
+                err0 += sqf(d0 - v);
+                err1 += sqf(d1 - v);
+            }
+            float be = err1;
+            if (err0 < err1) {
+                be = err0;
+                bq = q1i - 1;
+            }
+            total += be;
         }
         if (k < 8) q0 |= (uint32_t)bq << (4 * k);
         else q1 |= (uint32_t)bq << (4 * (k - 8));
-        total += be;
     }
-    return total;
+    return INT ? (float)itotal : total;
 }
 
 // block_quant<CH, BITS, PAIRS, true> walking each subset's pixels in turn,
@@ -347,7 +380,7 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
 template <int CH, int BITS, int PAIRS, class B>
 BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
     constexpr int levels = 1 << BITS;
-    float total = 0.0f;
+    int total = 0;
     q0 = 0;
     q1 = 0;
 #pragma unroll
@@ -373,16 +406,10 @@ BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t patt
             proj = fmaf(fmaf(-q, div, proj), rdv, q);
             int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
             int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
-            float err0 = 0.0f, err1 = 0.0f;
+            int err0 = 0, err1 = 0;
 #pragma unroll
-            for (int p = 0; p < CH; p++) {
-                float v = blk(p, k);
-                float d0 = (float)((uint32_t)(base[p] + w0 * dif[p]) >> 6);
-                float d1 = (float)((uint32_t)(base[p] + w1 * dif[p]) >> 6);
-                err0 += sqf(d0 - v);
-                err1 += sqf(d1 - v);
-            }
-            float be = err1;
+            for (int p = 0; p < CH; p++) pixel_err2(base[p], dif[p], blk(p, k), w0, w1, err0, err1);
+            int be = err1;
             uint32_t bq = (uint32_t)q1i;
             if (err0 < err1) {
                 be = err0;
@@ -393,7 +420,7 @@ BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t patt
             total += be;
         }
     }
-    return total;
+    return (float)total;
 }
 
 // common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH).
