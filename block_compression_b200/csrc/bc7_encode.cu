@@ -36,7 +36,7 @@
 
 // Minimum resident CTAs per SM requested from the register allocator.
 #ifndef BCN_MODE45_MINB
-#define BCN_MODE45_MINB 5
+#define BCN_MODE45_MINB 6
 #endif
 #ifndef BCN_REFINE_MINB
 #define BCN_REFINE_MINB 4
@@ -45,10 +45,10 @@
 #define BCN_PREP_MINB 4
 #endif
 #ifndef BCN_SEARCH_MINB  // search of modes 0-3
-#define BCN_SEARCH_MINB 5
+#define BCN_SEARCH_MINB 6
 #endif
 #ifndef BCN_SEARCH7_MINB  // mode 7 (4 channels) needs more registers
-#define BCN_SEARCH7_MINB 4
+#define BCN_SEARCH7_MINB 5
 #endif
 namespace bcn {
 namespace bc7 {

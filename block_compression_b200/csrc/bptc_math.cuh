@@ -273,6 +273,46 @@ BCN_DEV void pixel_err2(int bs, int df, float v, int w0, int w1, int& err0, int&
     err1 += a1 * a1;
 }
 
+// One pixel of block_quant's integer path (pixels and endpoints bytes):
+// vi the pixel's channels, ia / df the pair's low endpoint and
+// high - low endpoint per channel, dv / rdv the pair's squared length and
+// its reciprocal. With t = v - ia every projection term t * df is an exact
+// integer and so is their sum (at most 4 * 255^2): the float sum the
+// reference forms is that integer. The quotient by dv is the reciprocal and
+// one fused correction step (exact for all such integer pairs), and the
+// decoded-value errors are pixel_err2's with bs - 64 * v = 32 - 64 * t.
+// Returns the chosen index; be = its squared error.
+template <int CH, int BITS>
+BCN_DEV int fit_pixel_int(const int* vi, const int* ia, const int* df, float dv, float rdv, int& be) {
+    constexpr int levels = 1 << BITS;
+    int t[CH], pi = 0;
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        t[p] = vi[p] - ia[p];
+        pi += t[p] * df[p];
+    }
+    float proj = (float)pi;
+    const float q = proj * rdv;
+    proj = fmaf(fmaf(-q, dv, proj), rdv, q);
+    const int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
+    const int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
+    int err0 = 0, err1 = 0;
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        const int bsv = 32 - 64 * t[p];
+        const int a0 = (bsv + w0 * df[p]) >> 6, a1 = (bsv + w1 * df[p]) >> 6;
+        err0 += a0 * a0;
+        err1 += a1 * a1;
+    }
+    be = err1;
+    int bq = q1i;
+    if (err0 < err1) {
+        be = err0;
+        bq = q1i - 1;
+    }
+    return bq;
+}
+
 // common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8, dequantised
 // values in [0, 255]. Everything that depends only on the pair is computed
 // once per pair with the reference's own operations (so the per-pixel values
@@ -286,8 +326,49 @@ BCN_DEV void pixel_err2(int bs, int df, float v, int w0, int w1, int& err0, int&
 // exhaustively by the oracle test). Otherwise IEEE division (BC6H).
 template <int CH, int BITS, int PAIRS, bool INT = false, class B>
 BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
+    if (INT) {
+        int ia[PAIRS][CH], df[PAIRS][CH];
+        float dv[PAIRS], rdv[PAIRS];
+#pragma unroll
+        for (int j = 0; j < PAIRS; j++) {
+            float div = 0.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                const float d = ep[8 * j + 4 + p] - ep[8 * j + p];
+                div += sqf(d);
+                ia[j][p] = (int)ep[8 * j + p];
+                df[j][p] = (int)ep[8 * j + 4 + p] - ia[j][p];
+            }
+            dv[j] = div;
+            rdv[j] = __frcp_rn(div);
+        }
+        int total = 0;
+        q0 = 0;
+        q1 = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int j = PAIRS == 1 ? 0 : (int)((pattern >> (2 * k)) & 3);
+            int vi[CH], a[CH], f[CH];
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                // indices stay inside the PAIRS rows
+                vi[p] = (int)blk(p, k);
+                a[p] = sel_pair<PAIRS>(j, ia[0][p], ia[PAIRS > 1 ? 1 : 0][p], ia[PAIRS > 2 ? 2 : 0][p]);
+                f[p] = sel_pair<PAIRS>(j, df[0][p], df[PAIRS > 1 ? 1 : 0][p], df[PAIRS > 2 ? 2 : 0][p]);
+            }
+            int be;
+            const uint32_t bq = (uint32_t)fit_pixel_int<CH, BITS>(
+                vi, a, f, sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]),
+                sel_pair<PAIRS>(j, rdv[0], rdv[PAIRS > 1 ? 1 : 0], rdv[PAIRS > 2 ? 2 : 0]), be);
+            if (k < 8) q0 |= bq << (4 * k);
+            else q1 |= bq << (4 * (k - 8));
+            total += be;
+        }
+        return (float)total;
+    }
+    // float path (BC6H): IEEE division
     constexpr int levels = 1 << BITS;
-    float dd[PAIRS][CH], dv[PAIRS], rdv[PAIRS];
+    float dd[PAIRS][CH], dv[PAIRS];
     int base[PAIRS][CH], dif[PAIRS][CH];
 #pragma unroll
     for (int j = 0; j < PAIRS; j++) {
@@ -301,10 +382,8 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
             dif[j][p] = ib - ia;
         }
         dv[j] = div;
-        rdv[j] = INT ? __frcp_rn(div) : 0.0f;
     }
     float total = 0.0f;
-    int itotal = 0;
     q0 = 0;
     q1 = 0;
 #pragma unroll
@@ -318,57 +397,31 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
             float d = sel_pair<PAIRS>(j, dd[0][p], dd[PAIRS > 1 ? 1 : 0][p], dd[PAIRS > 2 ? 2 : 0][p]);
             proj += (blk(p, k) - ea) * d;
         }
-        {
-            const float y = sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
-            if (INT) {
-                const float r = sel_pair<PAIRS>(j, rdv[0], rdv[PAIRS > 1 ? 1 : 0], rdv[PAIRS > 2 ? 2 : 0]);
-                const float q = proj * r;
-                proj = fmaf(fmaf(-q, y, proj), r, q);
-            } else {
-                proj /= y;
-            }
-        }
+        proj /= sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]);
         int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
         int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
+        float err0 = 0.0f, err1 = 0.0f;
+#pragma unroll
+        for (int p = 0; p < CH; p++) {
+            int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
+            int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
+            float v = blk(p, k);
+            float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
+            float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
+            err0 += sqf(d0 - v);
+            err1 += sqf(d1 - v);
+        }
+        float be = err1;
         int bq = q1i;
-        if (INT) {
-            // integer pixel errors, see pixel_err2
-            int err0 = 0, err1 = 0;
-#pragma unroll
-            for (int p = 0; p < CH; p++) {
-                int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
-                int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
-                pixel_err2(bs, df, blk(p, k), w0, w1, err0, err1);
-            }
-            int be = err1;
-            if (err0 < err1) {
-                be = err0;
-                bq = q1i - 1;
-            }
-            itotal += be;
-        } else {
-            float err0 = 0.0f, err1 = 0.0f;
-#pragma unroll
-            for (int p = 0; p < CH; p++) {
-                int bs = sel_pair<PAIRS>(j, base[0][p], base[PAIRS > 1 ? 1 : 0][p], base[PAIRS > 2 ? 2 : 0][p]);
-                int df = sel_pair<PAIRS>(j, dif[0][p], dif[PAIRS > 1 ? 1 : 0][p], dif[PAIRS > 2 ? 2 : 0][p]);
-                float v = blk(p, k);
-                float d0 = (float)((uint32_t)(bs + w0 * df) >> 6);
-                float d1 = (float)((uint32_t)(bs + w1 * df) >> 6);
-                err0 += sqf(d0 - v);
-                err1 += sqf(d1 - v);
-            }
-            float be = err1;
-            if (err0 < err1) {
-                be = err0;
-                bq = q1i - 1;
-            }
-            total += be;
+        if (err0 < err1) {
+            be = err0;
+            bq = q1i - 1;
         }
         if (k < 8) q0 |= (uint32_t)bq << (4 * k);
         else q1 |= (uint32_t)bq << (4 * (k - 8));
+        total += be;
     }
-    return INT ? (float)itotal : total;
+    return total;
 }
 
 // block_quant<CH, BITS, PAIRS, true> walking each subset's pixels in turn,
@@ -379,42 +432,29 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
 // Meant for a pattern shared by the whole warp (no divergent loops).
 template <int CH, int BITS, int PAIRS, class B>
 BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
-    constexpr int levels = 1 << BITS;
     int total = 0;
     q0 = 0;
     q1 = 0;
 #pragma unroll
     for (int j = 0; j < PAIRS; j++) {
-        float dd[CH], div = 0.0f;
-        int base[CH], dif[CH];
+        int ia[CH], df[CH];
+        float div = 0.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
-            dd[p] = ep[8 * j + 4 + p] - ep[8 * j + p];
-            div += sqf(dd[p]);
-            int ia = (int)ep[8 * j + p], ib = (int)ep[8 * j + 4 + p];
-            base[p] = ia * 64 + 32;
-            dif[p] = ib - ia;
+            const float d = ep[8 * j + 4 + p] - ep[8 * j + p];
+            div += sqf(d);
+            ia[p] = (int)ep[8 * j + p];
+            df[p] = (int)ep[8 * j + 4 + p] - ia[p];
         }
         const float rdv = __frcp_rn(div);
         const uint32_t mask = PAIRS == 1 ? 0xFFFFu : subset_mask_from_map(pattern, j);
         for (uint32_t m = mask; m; m &= m - 1) {
             const int k = __ffs(m) - 1;
-            float proj = 0.0f;
+            int vi[CH];
 #pragma unroll
-            for (int p = 0; p < CH; p++) proj += (blk(p, k) - ep[8 * j + p]) * dd[p];
-            const float q = proj * rdv;
-            proj = fmaf(fmaf(-q, div, proj), rdv, q);
-            int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
-            int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
-            int err0 = 0, err1 = 0;
-#pragma unroll
-            for (int p = 0; p < CH; p++) pixel_err2(base[p], dif[p], blk(p, k), w0, w1, err0, err1);
-            int be = err1;
-            uint32_t bq = (uint32_t)q1i;
-            if (err0 < err1) {
-                be = err0;
-                bq = (uint32_t)(q1i - 1);
-            }
+            for (int p = 0; p < CH; p++) vi[p] = (int)blk(p, k);
+            int be;
+            const uint32_t bq = (uint32_t)fit_pixel_int<CH, BITS>(vi, ia, df, div, rdv, be);
             if (k < 8) q0 |= bq << (4 * k);
             else q1 |= bq << (4 * (k - 8));
             total += be;
