@@ -152,7 +152,7 @@ BCN_DEV float eval_part(const B& blk, const uint32_t* map, int part_id, int qep[
         const uint32_t m1 = subset_mask_from_map(pattern, 1), m0 = ~m1 & 0xFFFFu;
         const bool small1 = __popc(m1) <= 8;
         float ss[15], st[15];
-        stats_masked<T::ch>(blk, small1 ? m1 : m0, ss);
+        stats_masked<T::ch, true>(blk, small1 ? m1 : m0, ss);
 #pragma unroll
         for (int i = 0; i < 15; i++) st[i] = small1 ? full[i * NB] - ss[i] : ss[i];
         block_segment_from_stats<T::ch, true, true>(blk, m0, st, ep);
@@ -252,7 +252,7 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
         for (int i = 0; i < 24; i++) ep[i] = 0.0f;
 #pragma unroll
         for (int j = 0; j < T::pairs; j++)
-            opt_endpoints<T::ch, T::bits>(ep + 8 * j, blk, bq0, bq1, subset_mask_from_map(pattern, j));
+            opt_endpoints<T::ch, T::bits, true>(ep + 8 * j, blk, bq0, bq1, subset_mask_from_map(pattern, j));
     }
     if (MODE != 7) best_err += opaque_err;
     int best_qep[24];
@@ -323,9 +323,9 @@ BCN_DEV void channel_opt_endpoints(float ep[2], const C& cb, int bits, uint32_t 
         float q = (float)(((k < 8 ? q0 : q1) >> (4 * (k & 7))) & 15);
         float x = lm1 - q;
         sum_q += q;
-        sum_qq += q * q;
+        sum_qq = mac<true>(sum_qq, q, q);
         sum += cb[k];
-        atb1 += x * cb[k];
+        atb1 = mac<true>(atb1, x, cb[k]);
     }
     float atb2 = lm1 * sum - atb1;
     float cxx = 16.0f * sqf(lm1) - 2.0f * lm1 * sum_q + sum_qq;
@@ -424,7 +424,7 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
         for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
         err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
         if (it == refine) break;
-        opt_endpoints<3, bits>(ep, cb, q0, q1, 0xFFFFu);
+        opt_endpoints<3, bits, true>(ep, cb, q0, q1, 0xFFFFu);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
     const Chan chan{pxlane + rot * 16 * NB};
@@ -472,7 +472,7 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
         for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
         err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
         if (it == refine) break;
-        opt_endpoints<CH, 4>(ep, blk, q0, q1, 0xFFFFu);
+        opt_endpoints<CH, 4, true>(ep, blk, q0, q1, 0xFFFFu);
     }
     out = code_mode6(qep, q0, q1);
     return err;

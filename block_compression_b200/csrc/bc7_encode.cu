@@ -209,10 +209,10 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
         // 3-channel ones (entries 0-2, 4, 5, 7, 10-12, 14 are the same sums
         // in the same order), so one pass per partition feeds both bounds.
         float full[15];
-        stats_masked<4>(blk, 0xFFFFu, full);
+        stats_masked<4, true>(blk, 0xFFFFu, full);
         for (int part = warp; part < 64; part += NW) {
             float st[15], cv[10];
-            stats_masked<4>(blk, subset_mask_from_map(kPartitionMap[part], 0), st);
+            stats_masked<4, true>(blk, subset_mask_from_map(kPartitionMap[part], 0), st);
             covar_from_stats<4, true>(cv, st);
             float ba = 0.0f, bb = 0.0f;
             ba += pca_bound<3>(cv);
@@ -228,8 +228,8 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
     } else if (P.bounds_a || P.bounds_b) {
         const int set = P.bounds_a ? 0 : 1;
         float full[15];
-        if (set == 0) stats_masked<3>(blk, 0xFFFFu, full);
-        else stats_masked<4>(blk, 0xFFFFu, full);
+        if (set == 0) stats_masked<3, true>(blk, 0xFFFFu, full);
+        else stats_masked<4, true>(blk, 0xFFFFu, full);
         for (int part = warp; part < 64; part += NW) {
             uint32_t mask = subset_mask_from_map(kPartitionMap[part], 0);
             float b12 = set == 0 ? pca_bound_split<3, true>(blk, mask, full) : pca_bound_split<4, true>(blk, mask, full);

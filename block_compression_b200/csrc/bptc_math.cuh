@@ -27,9 +27,18 @@ BCN_DEV int unquant_w(int bits, int i) {
 
 BCN_DEV float sel3(int j, float a, float b, float c) { return j == 0 ? a : (j == 1 ? b : c); }
 
+// Product-accumulate acc + x * y of the statistics. INT: x, y and acc are
+// integers whose products and sums stay below 2^24 (8-bit pixels, at most
+// 16 of them), so the product and the sum are exact either way and one fused
+// multiply-add gives the same number as the reference's multiply then add.
+template <bool INT>
+BCN_DEV float mac(float acc, float x, float y) {
+    return INT ? fmaf(x, y, acc) : acc + x * y;
+}
+
 // common.rs:294-332 over the set pixels only (adding the reference's +0.0
 // terms of unset pixels changes none of the non-negative sums).
-template <int CH, class B>
+template <int CH, bool INT = false, class B>
 BCN_DEV void stats_masked(const B& blk, uint32_t mask, float st[15]) {
 #pragma unroll
     for (int i = 0; i < 15; i++) st[i] = 0.0f;
@@ -40,19 +49,19 @@ BCN_DEV void stats_masked(const B& blk, uint32_t mask, float st[15]) {
         st[10] += r;
         st[11] += g;
         st[12] += b;
-        st[0] += r * r;
-        st[1] += r * g;
-        st[2] += r * b;
-        st[4] += g * g;
-        st[5] += g * b;
-        st[7] += b * b;
+        st[0] = mac<INT>(st[0], r, r);
+        st[1] = mac<INT>(st[1], r, g);
+        st[2] = mac<INT>(st[2], r, b);
+        st[4] = mac<INT>(st[4], g, g);
+        st[5] = mac<INT>(st[5], g, b);
+        st[7] = mac<INT>(st[7], b, b);
         if (CH == 4) {
             float a = blk(3, k);
             st[13] += a;
-            st[3] += r * a;
-            st[6] += g * a;
-            st[8] += b * a;
-            st[9] += a * a;
+            st[3] = mac<INT>(st[3], r, a);
+            st[6] = mac<INT>(st[6], g, a);
+            st[8] = mac<INT>(st[8], b, a);
+            st[9] = mac<INT>(st[9], a, a);
         }
     }
 }
@@ -158,7 +167,7 @@ BCN_DEV float pca_bound(const float cv[10]) {
 template <int CH, bool INT = false>
 BCN_DEV float pca_bound_split(const Blk& blk, uint32_t mask, const float full[15]) {
     float st[15], cv[10];
-    stats_masked<CH>(blk, mask, st);
+    stats_masked<CH, INT>(blk, mask, st);
     covar_from_stats<CH, INT>(cv, st);
     float b = 0.0f;
     b += pca_bound<CH>(cv);
@@ -172,7 +181,8 @@ BCN_DEV float pca_bound_split(const Blk& blk, uint32_t mask, const float full[15
 // Entry e of stats_masked<CH>(blk, 0xFFFF, st) alone: 0-9 the channel
 // products (r*r, r*g, r*b, r*a, g*g, g*b, g*a, b*b, b*a, a*a), 10-13 the
 // channel sums, 14 the pixel count; entries of alpha stay 0 when CH = 3.
-// Summed over all 16 pixels in order, the same as stats_masked.
+// Summed over all 16 pixels in order, the same as stats_masked (8-bit
+// pixels: exact integer sums).
 template <int CH, class B>
 BCN_DEV float stat_entry(const B& blk, int e) {
     if (e == 14) return 16.0f;
@@ -185,7 +195,7 @@ BCN_DEV float stat_entry(const B& blk, int e) {
         for (int k = 0; k < 16; k++) acc += blk(ca, k);
     } else {
 #pragma unroll
-        for (int k = 0; k < 16; k++) acc += blk(ca, k) * blk(cb, k);
+        for (int k = 0; k < 16; k++) acc = mac<true>(acc, blk(ca, k), blk(cb, k));
     }
     return acc;
 }
@@ -237,7 +247,7 @@ BCN_DEV void block_segment_from_stats(const B& blk, uint32_t mask, float st[15],
 template <int CH, bool CLAMP, bool INT = false, class B>
 BCN_DEV void block_segment(const B& blk, uint32_t mask, float ep[8]) {
     float st[15];
-    stats_masked<CH>(blk, mask, st);
+    stats_masked<CH, INT>(blk, mask, st);
     block_segment_from_stats<CH, CLAMP, INT>(blk, mask, st, ep);
 }
 
@@ -463,8 +473,9 @@ BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t patt
     return (float)total;
 }
 
-// common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH).
-template <int CH, int BITS, class B>
+// common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH). INT: 8-bit pixels
+// (the sums of index and pixel products are exact integers, see mac).
+template <int CH, int BITS, bool INT = false, class B>
 BCN_DEV void opt_endpoints(float* ep, const B& blk, uint32_t q0, uint32_t q1, uint32_t mask) {
     constexpr int levels = 1 << BITS;
     const float lm1 = (float)(levels - 1);
@@ -476,13 +487,13 @@ BCN_DEV void opt_endpoints(float* ep, const B& blk, uint32_t q0, uint32_t q1, ui
         if (((mask >> k) & 1) == 0) continue;
         float x = lm1 - q;
         sum_q += q;
-        sum_qq += q * q;
+        sum_qq = mac<INT>(sum_qq, q, q);
         sum[4] += 1.0f;
 #pragma unroll
         for (int p = 0; p < CH; p++) {
             float v = blk(p, k);
             sum[p] += v;
-            atb1[p] += x * v;
+            atb1[p] = mac<INT>(atb1[p], x, v);
         }
     }
     float atb2[4];

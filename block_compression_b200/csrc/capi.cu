@@ -348,6 +348,69 @@ extern "C" int bc_compress_rgba16_device(const bc_bc6h_settings* settings, const
                           BC6H_SRC_RGBA16F, (cudaStream_t)stream);
 }
 
+// Streams and events of the pipelined host-buffer encode, per thread and
+// device (created on first use).
+struct HostPipe {
+    static constexpr int kRing = 4;
+    cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    cudaEvent_t ev_up[kRing] = {}, ev_comp[kRing] = {};
+    int device = -1;
+    void release() {
+        for (int i = 0; i < kRing; i++) {
+            if (ev_up[i]) cudaEventDestroy(ev_up[i]);
+            if (ev_comp[i]) cudaEventDestroy(ev_comp[i]);
+            ev_up[i] = ev_comp[i] = nullptr;
+        }
+        for (cudaStream_t* st : {&up, &comp, &down})
+            if (*st) {
+                cudaStreamDestroy(*st);
+                *st = nullptr;
+            }
+        device = -1;
+    }
+    ~HostPipe() { release(); }
+    int get() {
+        int dev = 0;
+        BC_CUDA(cudaGetDevice(&dev));
+        if (dev == device) return BC_OK;
+        release();
+        for (cudaStream_t* st : {&up, &comp, &down}) BC_CUDA(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+        for (int i = 0; i < kRing; i++) {
+            BC_CUDA(cudaEventCreateWithFlags(&ev_up[i], cudaEventDisableTiming));
+            BC_CUDA(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming));
+        }
+        device = dev;
+        return BC_OK;
+    }
+};
+static thread_local HostPipe t_pipe;
+
+// One band of host_encode: rows y0 .. y0 + h - 1 up, encoded, blocks down.
+static int enqueue_band(int variant, const void* settings, const uint8_t* src, uint8_t* dsrc, size_t stride_bytes,
+                        size_t bpp, uint8_t* blocks, uint8_t* ddst, uint32_t width, uint32_t y0, uint32_t h,
+                        size_t block_row_bytes, int bc6h_source, int ring) {
+    const size_t soff = (size_t)y0 * stride_bytes;
+    const size_t sbytes = (size_t)(h - 1) * stride_bytes + (size_t)width * bpp;
+    const size_t doff = (size_t)(y0 / 4) * block_row_bytes;
+    const size_t dbytes = (size_t)((h + 3) / 4) * block_row_bytes;
+    cudaEvent_t eu = t_pipe.ev_up[ring], ec = t_pipe.ev_comp[ring];
+    BC_CUDA(cudaMemcpyAsync(dsrc + soff, src + soff, sbytes, cudaMemcpyHostToDevice, t_pipe.up));
+    BC_CUDA(cudaEventRecord(eu, t_pipe.up));
+    BC_CUDA(cudaStreamWaitEvent(t_pipe.comp, eu, 0));
+    int rc = enqueue_encode(variant, settings, dsrc + soff, stride_bytes, width, h, ddst + doff, bc6h_source,
+                            t_pipe.comp);
+    if (rc != BC_OK) return rc;
+    BC_CUDA(cudaEventRecord(ec, t_pipe.comp));
+    BC_CUDA(cudaStreamWaitEvent(t_pipe.down, ec, 0));
+    BC_CUDA(cudaMemcpyAsync(blocks + doff, ddst + doff, dbytes, cudaMemcpyDeviceToHost, t_pipe.down));
+    return BC_OK;
+}
+
+// Host-buffer encode, pipelined: the image is cut into bands of whole block
+// rows (about 4 MiB of source each) and band i's upload, encode and download
+// run on three streams, so the copies of one band overlap the kernels of its
+// neighbours. Blocks are independent and every band but the last is a whole
+// number of block rows, so the bands' blocks are exactly the image's.
 static int host_encode(int variant, const void* settings, const uint8_t* src, size_t stride_bytes, size_t bpp,
                        uint8_t* blocks, uint32_t width, uint32_t height, int bc6h_source) {
     size_t src_bytes = (size_t)(height - 1) * stride_bytes + (size_t)width * bpp;
@@ -357,13 +420,29 @@ static int host_encode(int variant, const void* settings, const uint8_t* src, si
     if (rc != BC_OK) return rc;
     rc = t_staging.get(1, dst_bytes, &ddst);
     if (rc != BC_OK) return rc;
-    cudaStream_t s = 0;
-    BC_CUDA(cudaMemcpyAsync(dsrc, src, src_bytes, cudaMemcpyHostToDevice, s));
-    rc = enqueue_encode(variant, settings, (const uint8_t*)dsrc, stride_bytes, width, height, (uint8_t*)ddst,
-                        bc6h_source, s);
+    rc = t_pipe.get();
     if (rc != BC_OK) return rc;
-    BC_CUDA(cudaMemcpyAsync(blocks, ddst, dst_bytes, cudaMemcpyDeviceToHost, s));
-    BC_CUDA(cudaStreamSynchronize(s));
+    const size_t block_row_bytes = bc_blocks_byte_size(variant, width, 4);
+    const size_t band_target = (size_t)4 << 20;
+    uint32_t band_rows = (uint32_t)(band_target / (stride_bytes ? stride_bytes : 1)) & ~3u;
+    if (band_rows < 4) band_rows = 4;
+    const uint32_t nbands = (height + band_rows - 1) / band_rows;
+    int brc = BC_OK;
+    for (uint32_t b = 0; b < nbands && brc == BC_OK; b++) {
+        const uint32_t y0 = b * band_rows;
+        const uint32_t h = height - y0 < band_rows ? height - y0 : band_rows;
+        brc = enqueue_band(variant, settings, src, (uint8_t*)dsrc, stride_bytes, bpp, blocks, (uint8_t*)ddst, width,
+                           y0, h, block_row_bytes, bc6h_source, b % HostPipe::kRing);
+    }
+    // every band's copies have finished before the caller's buffers are
+    // released, on the error path too
+    cudaError_t e0 = cudaStreamSynchronize(t_pipe.up);
+    cudaError_t e1 = cudaStreamSynchronize(t_pipe.comp);
+    cudaError_t e2 = cudaStreamSynchronize(t_pipe.down);
+    if (brc != BC_OK) return brc;
+    BC_CUDA(e0);
+    BC_CUDA(e1);
+    BC_CUDA(e2);
     return BC_OK;
 }
 
