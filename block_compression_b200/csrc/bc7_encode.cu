@@ -238,17 +238,32 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
     }
     __syncthreads();
     // partial_sort_list: keys are unique, so the first K entries are the K
-    // smallest in ascending order.
+    // smallest in ascending order. Tournament selection: the minima of 8
+    // groups of 8 keys; each step takes the smallest group minimum (the low
+    // 6 bits of a key are its partition, so also its group) and rescans only
+    // that group.
     for (int set = 0; set < 2; set++) {
         int K = set == 0 ? P.k_a : P.k_b;
         if (K == 0 || warp != set) continue;
+        int gm[8];
+#pragma unroll
+        for (int g = 0; g < 8; g++) {
+            int m = INT_MAX;
+#pragma unroll
+            for (int i = 0; i < 8; i++) m = min(m, keys[set][8 * g + i][lane]);
+            gm[g] = m;
+        }
         for (int k = 0; k < K; k++) {
-            // the low 6 bits of a key are its partition
-            int best = INT_MAX;
-#pragma unroll 16
-            for (int q = 0; q < 64; q++) best = min(best, keys[set][q][lane]);
-            const int bi = best & 63;
+            int best = gm[0];
+#pragma unroll
+            for (int g = 1; g < 8; g++) best = min(best, gm[g]);
+            const int bi = best & 63, bg = bi >> 3;
             keys[set][bi][lane] = INT_MAX;
+            int m = INT_MAX;
+#pragma unroll
+            for (int i = 0; i < 8; i++) m = min(m, keys[set][8 * bg + i][lane]);
+#pragma unroll
+            for (int g = 0; g < 8; g++) gm[g] = g == bg ? m : gm[g];
             w.lists[(size_t)(set == 0 ? k : P.k_a + k) * w.npad + gi] = (uint8_t)bi;
         }
     }
