@@ -237,12 +237,16 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
     // strictly better result. One copy of the quantise + index-fit code.
 #pragma unroll 1
     for (uint32_t it = 0;; it++) {
-        int qep[24];
-        uint32_t q0, q1;
-        quant_dequant_part<MODE>(qep, ep);
+        uint32_t pk[6], q0, q1;
+        {
+            int qep[24];
+            quant_dequant_part<MODE>(qep, ep);
+            pack_qep<MODE>(pk, qep);  // 6 words live across the index fit instead of 24
+        }
         float err = block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
         if (it == 0 || err < best_err) {
-            pack_qep<MODE>(best_pk, qep);
+#pragma unroll
+            for (int i = 0; i < 6; i++) best_pk[i] = pk[i];
             bq0 = q0;
             bq1 = q1;
             if (it != 0) best_err = err;

@@ -41,6 +41,10 @@
 #ifndef BCN_REFINE_MINB
 #define BCN_REFINE_MINB 4
 #endif
+#ifndef BCN_REFINE_WARPS  // warps (tiles) per CTA of the refine and mode-6 kernels
+#define BCN_REFINE_WARPS 4
+#endif
+static_assert(BCN_REFINE_WARPS >= 1 && BCN_REFINE_WARPS <= 5, "8 KiB of static shared memory per warp, 48 KiB at most");
 #ifndef BCN_PREP_MINB
 #define BCN_PREP_MINB 4
 #endif
@@ -474,7 +478,7 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
     p += npad * 4 * nslots;
     w.lists = p;
 
-    constexpr int NWP = 8, NWR = 4, NW45 = 4;
+    constexpr int NWP = 8, NWR = BCN_REFINE_WARPS, NW45 = 4;
     bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
     auto groups = [](int count, int nw) { return (unsigned)((count + nw - 1) / nw); };
     const int modes[5] = {0, 2, 1, 3, 7};

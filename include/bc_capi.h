@@ -13,7 +13,11 @@
  *     legacy default stream). *_device entry points are stream-ordered and
  *     asynchronous: they validate arguments, enqueue kernels and return.
  *   - Host-pointer entry points (bc_compress_rgba8, ...) are synchronous and
- *     mirror the reference's CPU functions byte for byte.
+ *     mirror the reference's CPU functions byte for byte. The encoders cut
+ *     the image into bands of block rows (about 4 MiB of source each) and
+ *     overlap each band's upload and download with its neighbours' kernels
+ *     on library-owned streams; pinned (page-locked) host buffers let the
+ *     copies run asynchronously.
  *   - Output blocks are little-endian, in row-major block order, exactly as
  *     the reference writes them (src/encode.rs store_data).
  *   - All work runs on the CUDA device current on the calling thread.
