@@ -235,6 +235,9 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
     // Pass 0 re-creates the winner's state (its error is best_err already);
     // passes 1..iters fit the endpoints to the best indices and keep a
     // strictly better result. One copy of the quantise + index-fit code.
+    // A pass after which the best indices are unchanged is repeated exactly
+    // by every later pass (same endpoint-fit input, same outcome, and a
+    // repeat cannot be strictly better), so the loop stops there.
 #pragma unroll 1
     for (uint32_t it = 0;; it++) {
         uint32_t pk[6], q0, q1;
@@ -244,6 +247,7 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
             pack_qep<MODE>(pk, qep);  // 6 words live across the index fit instead of 24
         }
         float err = block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
+        const uint32_t pb0 = bq0, pb1 = bq1;
         if (it == 0 || err < best_err) {
 #pragma unroll
             for (int i = 0; i < 6; i++) best_pk[i] = pk[i];
@@ -251,7 +255,7 @@ BCN_DEV float refine_and_code(const B& blk, const uint32_t* map, int part_id, fl
             bq1 = q1;
             if (it != 0) best_err = err;
         }
-        if (it == iters) break;
+        if (it == iters || (it != 0 && bq0 == pb0 && bq1 == pb1)) break;
 #pragma unroll
         for (int i = 0; i < 24; i++) ep[i] = 0.0f;
 #pragma unroll
@@ -416,10 +420,12 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
     block_segment<3, true, true>(cb, 0xFFFFu, ep);
     // quantise + index fit, then `refine` times: endpoint fit, quantise +
     // index fit (one copy of each step in the code: the kernel is
-    // instruction-cache bound)
+    // instruction-cache bound). The endpoint fit depends only on the indices
+    // (and the pixels): once a pass returns the indices it was given, every
+    // later pass repeats it exactly, so the loop stops there.
     int qep[8];
     constexpr int EPB = MODE == 4 ? 5 : 7;
-    uint32_t q0, q1;
+    uint32_t q0, q1, p0 = 0, p1 = 0;
     float err;
 #pragma unroll 1
     for (uint32_t it = 0;; it++) {
@@ -427,7 +433,9 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)unpack_to_byte(qep[i], EPB);
         err = block_quant<3, bits, 1, true>(cb, ep, 0, q0, q1);
-        if (it == refine) break;
+        if (it == refine || (it != 0 && q0 == p0 && q1 == p1)) break;
+        p0 = q0;
+        p1 = q1;
         opt_endpoints<3, bits, true>(ep, cb, q0, q1, 0xFFFFu);
     }
     // scalar channel (opt_channel, bc7.rs:239-266)
@@ -439,13 +447,15 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
         aep[1] = fmaxf(aep[1], chan[k]);
     }
     int aqep[2];
-    uint32_t a0, a1;
+    uint32_t a0, a1, pa0 = 0, pa1 = 0;
     float aerr;
 #pragma unroll 1
-    for (uint32_t it = 0;; it++) {
+    for (uint32_t it = 0;; it++) {  // stops at a repeat, as above
         channel_quant_dequant(aqep, aep, aepbits);
         aerr = channel_opt_quant(a0, a1, chan, abits, aep);
-        if (it == refine_channel) break;
+        if (it == refine_channel || (it != 0 && a0 == pa0 && a1 == pa1)) break;
+        pa0 = a0;
+        pa1 = a1;
         channel_opt_endpoints(aep, chan, abits, a0, a1);
     }
     err += aerr;
@@ -465,9 +475,10 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
         ep[7] = 255.0f;
     }
     // quantise + index fit, then `refine` times: endpoint fit, quantise +
-    // index fit (one copy of each step in the code)
+    // index fit (one copy of each step in the code); stops at a pass that
+    // returns the indices it was given (every later pass would repeat it)
     int qep[8];
-    uint32_t q0, q1;
+    uint32_t q0, q1, p0 = 0, p1 = 0;
     float err;
 #pragma unroll 1
     for (uint32_t it = 0;; it++) {
@@ -475,7 +486,9 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
         err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
-        if (it == refine) break;
+        if (it == refine || (it != 0 && q0 == p0 && q1 == p1)) break;
+        p0 = q0;
+        p1 = q1;
         opt_endpoints<CH, 4, true>(ep, blk, q0, q1, 0xFFFFu);
     }
     out = code_mode6(qep, q0, q1);

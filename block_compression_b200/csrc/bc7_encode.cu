@@ -45,6 +45,9 @@
 #define BCN_REFINE_WARPS 4
 #endif
 static_assert(BCN_REFINE_WARPS >= 1 && BCN_REFINE_WARPS <= 5, "8 KiB of static shared memory per warp, 48 KiB at most");
+#ifndef BCN_MODE6_MINB
+#define BCN_MODE6_MINB 4
+#endif
 #ifndef BCN_PREP_MINB
 #define BCN_PREP_MINB 4
 #endif
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Wo
 
 // K5: mode 6 (bc7.rs:762-817), one warp per tile.
 template <int CH, int NW>
-__global__ void __launch_bounds__(NW * 32) bc7_mode6_kernel(Work w, uint32_t ntiles) {
+__global__ void __launch_bounds__(NW * 32, BCN_MODE6_MINB) bc7_mode6_kernel(Work w, uint32_t ntiles) {
     __shared__ float px[NW][64][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x * NW + warp;
