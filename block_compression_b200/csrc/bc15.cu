@@ -53,6 +53,8 @@ BCN_DEV void bc1_refine(const Px16& px, int pe[2], uint32_t bits, const float dc
     if ((bits ^ (bits * 4u)) < 4) {
         for (int p = 0; p < 3; p++) c0[p] = c1[p] = dc[p];
     } else {
+        // integer products and sums below 2^24: the fused multiply-adds give
+        // the reference's multiply-then-add results exactly
         float atb1[3] = {0.0f, 0.0f, 0.0f};
         float sum_q = 0.0f, sum_qq = 0.0f;
 #pragma unroll
@@ -60,10 +62,10 @@ BCN_DEV void bc1_refine(const Px16& px, int pe[2], uint32_t bits, const float dc
             float q = (float)((bits >> (2 * k)) & 3);
             float x = 3.0f - q;
             sum_q += q;
-            sum_qq += q * q;
-            atb1[0] += x * px.r[k];
-            atb1[1] += x * px.g[k];
-            atb1[2] += x * px.b[k];
+            sum_qq = fmaf(q, q, sum_qq);
+            atb1[0] = fmaf(x, px.r[k], atb1[0]);
+            atb1[1] = fmaf(x, px.g[k], atb1[1]);
+            atb1[2] = fmaf(x, px.b[k], atb1[2]);
         }
         float sum[3], atb2[3];
         for (int p = 0; p < 3; p++) {
@@ -105,16 +107,20 @@ BCN_DEV void bc1_core(const Px16& px, uint32_t& w0, uint32_t& w1) {
         for (int k = 0; k < 16; k++) acc += px.b[k];
         dc[2] = acc / 16.0f;
     }
+    // x = pixel - mean is n / 16 with |n| < 2^12 (the mean is a sum of 16
+    // bytes over 16), so every product x * y is n * m / 256 with
+    // |n * m| < 2^24: exact in f32. A fused multiply-add of an exact product
+    // rounds the sum once, exactly as the reference's multiply then add.
     float cv[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         float x0 = px.r[k] - dc[0], x1 = px.g[k] - dc[1], x2 = px.b[k] - dc[2];
-        cv[0] += x0 * x0;
-        cv[1] += x0 * x1;
-        cv[2] += x0 * x2;
-        cv[3] += x1 * x1;
-        cv[4] += x1 * x2;
-        cv[5] += x2 * x2;
+        cv[0] = fmaf(x0, x0, cv[0]);
+        cv[1] = fmaf(x0, x1, cv[1]);
+        cv[2] = fmaf(x0, x2, cv[2]);
+        cv[3] = fmaf(x1, x1, cv[3]);
+        cv[4] = fmaf(x1, x2, cv[4]);
+        cv[5] = fmaf(x2, x2, cv[5]);
     }
     const float eps = 1.1920929e-7f;  // f32::EPSILON
     cv[0] += eps;

@@ -475,10 +475,13 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
         ep[7] = 255.0f;
     }
     // quantise + index fit, then `refine` times: endpoint fit, quantise +
-    // index fit (one copy of each step in the code); stops at a pass that
-    // returns the indices it was given (every later pass would repeat it)
+    // index fit (one copy of each step in the code). A pass's input is the
+    // indices and, with 3 channels, the alpha endpoints it carries over (the
+    // endpoint fit writes channels 0-2 only); a pass whose output repeats its
+    // input is repeated exactly by every later pass, so the loop stops there.
     int qep[8];
     uint32_t q0, q1, p0 = 0, p1 = 0;
+    int pa0 = 0, pa1 = 0;
     float err;
 #pragma unroll 1
     for (uint32_t it = 0;; it++) {
@@ -486,9 +489,11 @@ BCN_DEV float mode6(const B& blk, uint32_t refine, uint4& out) {
 #pragma unroll
         for (int i = 0; i < 8; i++) ep[i] = (float)qep[i];
         err = block_quant<CH, 4, 1, true>(blk, ep, 0, q0, q1);
-        if (it == refine || (it != 0 && q0 == p0 && q1 == p1)) break;
+        if (it == refine || (it != 0 && q0 == p0 && q1 == p1 && qep[3] == pa0 && qep[7] == pa1)) break;
         p0 = q0;
         p1 = q1;
+        pa0 = qep[3];
+        pa1 = qep[7];
         opt_endpoints<CH, 4, true>(ep, blk, q0, q1, 0xFFFFu);
     }
     out = code_mode6(qep, q0, q1);
