@@ -467,7 +467,39 @@ namespace bc7 {
 
 // Carves the scratch arrays out of `scratch` and enqueues the pipeline over
 // `ntiles` tiles.
-static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int search_warps, cudaStream_t s) {
+// The second stream of run_pipeline, with its fork and join events; per
+// thread and device, created on first use.
+struct SideStream {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    int device = -1;
+    void release() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (st) cudaStreamDestroy(st);
+        fork = join = nullptr;
+        st = nullptr;
+        device = -1;
+    }
+    ~SideStream() { release(); }
+    cudaError_t get() {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess || dev == device) return e;
+        release();
+        // non-blocking: no implicit ordering with the legacy default stream,
+        // only the explicit fork / join events
+        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming)) != cudaSuccess) return e;
+        device = dev;
+        return cudaSuccess;
+    }
+};
+static thread_local SideStream t_side;
+
+static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int search_warps, cudaStream_t s,
+                                bool side_stream) {
     const Plan P = make_plan(w.S);
     size_t npad = (size_t)ntiles * NB;
     int nslots = 5 + P.n45_4 + P.n45_5 + 1;
@@ -482,8 +514,40 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
     w.lists = p;
 
     constexpr int NWP = 8, NWR = BCN_REFINE_WARPS, NW45 = 4;
-    bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
     auto groups = [](int count, int nw) { return (unsigned)((count + nw - 1) / nw); };
+    unsigned rgrid = (ntiles + NWR - 1) / NWR;
+    // The mode-4/5 and mode-6 candidates read only the tile and write their
+    // own result slots: on the second stream they overlap the prep / search
+    // / refine chain and fill the SMs its launches' last waves leave idle.
+    cudaStream_t s2 = s;
+    if (side_stream && (P.n45_5 || P.run6)) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaError_t e = cudaStreamIsCapturing(s, &cs);
+        if (e != cudaSuccess) return e;
+        if (cs == cudaStreamCaptureStatusNone) {
+            if ((e = t_side.get()) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(t_side.fork, s)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(t_side.st, t_side.fork, 0)) != cudaSuccess) return e;
+            s2 = t_side.st;
+        }
+    }
+    if (P.n45_5) {
+        dim3 g45(ntiles, groups(P.n45_5, NW45));
+        if (w.S.channels == 4) {
+            bc7_mode45_kernel<4, 0, true, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+            bc7_mode45_kernel<4, 1, true, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+            bc7_mode45_kernel<5, 0, true, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+        } else {
+            bc7_mode45_kernel<4, 0, false, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+            bc7_mode45_kernel<4, 1, false, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+            bc7_mode45_kernel<5, 0, false, NW45><<<g45, NW45 * 32, 0, s2>>>(w);
+        }
+    }
+    if (P.run6) {
+        if (w.S.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
+        else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
+    }
+    bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
     const int modes[5] = {0, 2, 1, 3, 7};
     for (int mi = 0; mi < 5; mi++) {
         if (!P.count[mi]) continue;
@@ -507,27 +571,15 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
             }
         }
     }
-    unsigned rgrid = (ntiles + NWR - 1) / NWR;
     if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (P.n45_5) {
-        dim3 g45(ntiles, groups(P.n45_5, NW45));
-        if (w.S.channels == 4) {
-            bc7_mode45_kernel<4, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-            bc7_mode45_kernel<4, 1, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-            bc7_mode45_kernel<5, 0, true, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-        } else {
-            bc7_mode45_kernel<4, 0, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-            bc7_mode45_kernel<4, 1, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-            bc7_mode45_kernel<5, 0, false, NW45><<<g45, NW45 * 32, 0, s>>>(w);
-        }
-    }
-    if (P.run6) {
-        if (w.S.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-        else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    if (s2 != s) {
+        cudaError_t e = cudaEventRecord(t_side.join, s2);
+        if (e != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, t_side.join, 0)) != cudaSuccess) return e;
     }
     bc7_select_kernel<<<(ntiles + 7) / 8, 256, 0, s>>>(w, ntiles);
     return cudaGetLastError();
@@ -536,7 +588,7 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
 }  // namespace bc7
 
 cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
-                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s) {
+                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s, bool side_stream) {
     using namespace bc7;
     uint32_t n = bw * bh;
     if (n == 0) return cudaSuccess;
@@ -550,7 +602,7 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
     w.tasks = nullptr;
     w.tile_task = nullptr;
     w.S = settings;
-    return run_pipeline(w, (n + NB - 1) / NB, scratch, 8, s);
+    return run_pipeline(w, (n + NB - 1) / NB, scratch, 8, s, side_stream);
 }
 
 cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
@@ -562,7 +614,7 @@ cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_tas
     w.tasks = tasks_dev;
     w.tile_task = tile_task_dev;
     w.S = settings;
-    return run_pipeline(w, ntiles, scratch, search_warps, s);
+    return run_pipeline(w, ntiles, scratch, search_warps, s, false);
 }
 
 }  // namespace bcn
@@ -633,7 +685,9 @@ extern "C" int bc_compress_bc7_device_noalloc(const bc_bc7_settings* settings, c
     void* scratch = nullptr;
     rc = noalloc_scratch_address(&scratch);
     if (rc != BC_OK) return rc;
-    cudaError_t e = launch_bc7_encode(rgba_dev, stride_bytes, bw, bh, blocks_dev, s7, scratch, (cudaStream_t)stream);
+    // single stream: this entry point creates no resources
+    cudaError_t e =
+        launch_bc7_encode(rgba_dev, stride_bytes, bw, bh, blocks_dev, s7, scratch, (cudaStream_t)stream, false);
     if (e != cudaSuccess) {
         record_cuda_error(e);
         return BC_ERR_CUDA;

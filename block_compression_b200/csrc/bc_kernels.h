@@ -47,8 +47,12 @@ void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_
 // BC7 runs as a short pipeline of kernels that exchange per-block state
 // through `scratch` (device memory of at least bc7_scratch_bytes()).
 size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& settings);
+// side_stream: run the mode-4/5 and mode-6 candidates on a library-owned
+// second stream forked from `s` and joined before the final selection (not
+// while `s` is capturing a graph).
 cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
-                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s);
+                              const BC7SettingsDev& settings, void* scratch, cudaStream_t s,
+                              bool side_stream = true);
 // Batched form: the pipeline over `ntiles` tiles of several regions
 // (tasks_dev / tile_task_dev in device memory). search_warps: 4 or 8
 // candidates per CTA in the search launches.
