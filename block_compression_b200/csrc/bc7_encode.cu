@@ -9,7 +9,7 @@
 // instruction cache: every warp of an SM ran a different mode):
 //
 //   prep     PCA split bounds of the 64 partitions, ascending top-k lists
-//            (modes 1/3/7); argmin keys initialised
+//            (modes 1/3/7)
 //   search   one launch per mode 0/2/1/3/7; grid (tile, candidate group), a
 //            warp evaluates one partition candidate for 32 blocks; the first
 //            minimum per block is kept with a 64-bit atomicMin on
@@ -19,6 +19,9 @@
 //   mode6    one warp per tile
 //   select   the reference's sequential "strictly better" scan over the
 //            per-mode results -> one 128-bit store per block
+//
+// mode4/5 + mode6, search/refine of modes 0/2, and prep -> search/refine of
+// modes 1/3/7 are independent chains, run on three streams.
 //
 // Blocks are staged in shared memory as planar f32 with 128-bit coalesced
 // loads. Every per-candidate computation keeps the reference's operation
@@ -200,7 +203,7 @@ BCN_DEV float opaque_err(const B& blk, uint32_t channels) {
 }
 
 // K1: PCA split bounds + ascending top-k partition lists (bc7.rs:622-655,
-// 819-851; common.rs:126-140), and argmin-key initialisation.
+// 819-851; common.rs:126-140).
 template <int NW>
 __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w) {
     __shared__ float px[64][NB];
@@ -274,8 +277,6 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
             w.lists[(size_t)(set == 0 ? k : P.k_a + k) * w.npad + gi] = (uint8_t)bi;
         }
     }
-    if (warp == NW - 1)
-        for (int m = 0; m < 5; m++) w.keys[(size_t)m * w.npad + gi] = ~0ull;
 }
 
 BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
@@ -467,18 +468,23 @@ namespace bc7 {
 
 // Carves the scratch arrays out of `scratch` and enqueues the pipeline over
 // `ntiles` tiles.
-// The second stream of run_pipeline, with its fork and join events; per
-// thread and device, created on first use.
+// The second and third streams of run_pipeline, with their fork and join
+// events; per thread and device, created on first use.
 struct SideStream {
-    cudaStream_t st = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t st = nullptr, st2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     int device = -1;
     void release() {
-        if (fork) cudaEventDestroy(fork);
-        if (join) cudaEventDestroy(join);
-        if (st) cudaStreamDestroy(st);
-        fork = join = nullptr;
-        st = nullptr;
+        for (cudaEvent_t* ev : {&fork, &join, &join2})
+            if (*ev) {
+                cudaEventDestroy(*ev);
+                *ev = nullptr;
+            }
+        for (cudaStream_t* q : {&st, &st2})
+            if (*q) {
+                cudaStreamDestroy(*q);
+                *q = nullptr;
+            }
         device = -1;
     }
     ~SideStream() { release(); }
@@ -489,9 +495,10 @@ struct SideStream {
         release();
         // non-blocking: no implicit ordering with the legacy default stream,
         // only the explicit fork / join events
-        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
-        if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess) return e;
-        if ((e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming)) != cudaSuccess) return e;
+        for (cudaStream_t* q : {&st, &st2})
+            if ((e = cudaStreamCreateWithFlags(q, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        for (cudaEvent_t* ev : {&fork, &join, &join2})
+            if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return e;
         device = dev;
         return cudaSuccess;
     }
@@ -516,11 +523,18 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
     constexpr int NWP = 8, NWR = BCN_REFINE_WARPS, NW45 = 4;
     auto groups = [](int count, int nw) { return (unsigned)((count + nw - 1) / nw); };
     unsigned rgrid = (ntiles + NWR - 1) / NWR;
-    // The mode-4/5 and mode-6 candidates read only the tile and write their
-    // own result slots: on the second stream they overlap the prep / search
-    // / refine chain and fill the SMs its launches' last waves leave idle.
-    cudaStream_t s2 = s;
-    if (side_stream && (P.n45_5 || P.run6)) {
+    // argmin keys of the five searches: all ones = no candidate yet
+    {
+        cudaError_t e = cudaMemsetAsync(w.keys, 0xFF, npad * 8 * 5, s);
+        if (e != cudaSuccess) return e;
+    }
+    // Three chains that only meet at the selection: mode 4/5 + mode 6 (read
+    // only the tile), modes 0/2 (search + refine over the fixed partition
+    // order) and prep -> modes 1/3/7. On their own streams (forked here,
+    // joined before the selection) their launches overlap and fill the SMs
+    // each launch's last wave leaves idle.
+    cudaStream_t s2 = s, s3 = s;
+    if (side_stream) {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaError_t e = cudaStreamIsCapturing(s, &cs);
         if (e != cudaSuccess) return e;
@@ -528,7 +542,9 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
             if ((e = t_side.get()) != cudaSuccess) return e;
             if ((e = cudaEventRecord(t_side.fork, s)) != cudaSuccess) return e;
             if ((e = cudaStreamWaitEvent(t_side.st, t_side.fork, 0)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(t_side.st2, t_side.fork, 0)) != cudaSuccess) return e;
             s2 = t_side.st;
+            s3 = t_side.st2;
         }
     }
     if (P.n45_5) {
@@ -547,32 +563,36 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
         if (w.S.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
         else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
     }
-    bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);  // also initialises the argmin keys
-    const int modes[5] = {0, 2, 1, 3, 7};
-    for (int mi = 0; mi < 5; mi++) {
-        if (!P.count[mi]) continue;
+    auto search = [&](int mi, cudaStream_t st) {
+        const int mode = mi == 0 ? 0 : (mi == 1 ? 2 : (mi == 2 ? 1 : (mi == 3 ? 3 : 7)));
         if (search_warps == 4) {
             dim3 g(ntiles, groups(P.count[mi], 4));
-            switch (modes[mi]) {
-                case 0: bc7_search_kernel<0, 4><<<g, 128, 0, s>>>(w); break;
-                case 2: bc7_search_kernel<2, 4><<<g, 128, 0, s>>>(w); break;
-                case 1: bc7_search_kernel<1, 4><<<g, 128, 0, s>>>(w); break;
-                case 3: bc7_search_kernel<3, 4><<<g, 128, 0, s>>>(w); break;
-                default: bc7_search_kernel<7, 4><<<g, 128, 0, s>>>(w); break;
+            switch (mode) {
+                case 0: bc7_search_kernel<0, 4><<<g, 128, 0, st>>>(w); break;
+                case 2: bc7_search_kernel<2, 4><<<g, 128, 0, st>>>(w); break;
+                case 1: bc7_search_kernel<1, 4><<<g, 128, 0, st>>>(w); break;
+                case 3: bc7_search_kernel<3, 4><<<g, 128, 0, st>>>(w); break;
+                default: bc7_search_kernel<7, 4><<<g, 128, 0, st>>>(w); break;
             }
         } else {
             dim3 g(ntiles, groups(P.count[mi], 8));
-            switch (modes[mi]) {
-                case 0: bc7_search_kernel<0, 8><<<g, 256, 0, s>>>(w); break;
-                case 2: bc7_search_kernel<2, 8><<<g, 256, 0, s>>>(w); break;
-                case 1: bc7_search_kernel<1, 8><<<g, 256, 0, s>>>(w); break;
-                case 3: bc7_search_kernel<3, 8><<<g, 256, 0, s>>>(w); break;
-                default: bc7_search_kernel<7, 8><<<g, 256, 0, s>>>(w); break;
+            switch (mode) {
+                case 0: bc7_search_kernel<0, 8><<<g, 256, 0, st>>>(w); break;
+                case 2: bc7_search_kernel<2, 8><<<g, 256, 0, st>>>(w); break;
+                case 1: bc7_search_kernel<1, 8><<<g, 256, 0, st>>>(w); break;
+                case 3: bc7_search_kernel<3, 8><<<g, 256, 0, st>>>(w); break;
+                default: bc7_search_kernel<7, 8><<<g, 256, 0, st>>>(w); break;
             }
         }
-    }
-    if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
+    };
+    // modes 0 and 2 search partitions in table order: no prep needed
+    if (P.count[0]) search(0, s3);
+    if (P.count[1]) search(1, s3);
+    if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
+    if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
+    bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);
+    for (int mi = 2; mi < 5; mi++)
+        if (P.count[mi]) search(mi, s);
     if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
     if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
@@ -580,6 +600,8 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
         cudaError_t e = cudaEventRecord(t_side.join, s2);
         if (e != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s, t_side.join, 0)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(t_side.join2, s3)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, t_side.join2, 0)) != cudaSuccess) return e;
     }
     bc7_select_kernel<<<(ntiles + 7) / 8, 256, 0, s>>>(w, ntiles);
     return cudaGetLastError();
