@@ -13,18 +13,22 @@ namespace bc7 {
 using namespace bptc;
 
 // Mode 4/5 candidate block (bc7.rs:680-696): channel `rot` replaced by alpha
-// (4-channel settings) or by 255 (3-channel settings).
+// (4-channel settings) or by 255 (3-channel settings, whose kernel fills the
+// staged alpha row with 255 first), so channel c reads row o[c]: its own or
+// the alpha row, chosen once per candidate. Volatile reads: every use is a
+// shared-memory load, so the compiler keeps no register copy of the block
+// across the refinement loops (which cost this long kernel spills).
 template <bool CH4>
 struct BlkRot {
     const float* p;
-    int rot;
-    // volatile reads: every use is a shared-memory load, so the compiler
-    // keeps no register copy of the block across the refinement loops
-    // (which cost this long kernel spills)
+    int o[3];
+    BCN_DEV BlkRot(const float* pxlane, int rot) : p(pxlane) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) o[c] = (c == rot ? 48 : c * 16) * NB;
+    }
     BCN_DEV float operator()(int c, int k) const {
-        const volatile float* q = p;
-        if (c == rot) return CH4 ? q[(48 + k) * NB] : 255.0f;
-        return q[(c * 16 + k) * NB];
+        const volatile float* q = p + o[c];
+        return q[k * NB];
     }
 };
 
@@ -415,7 +419,7 @@ BCN_DEV float mode45_candidate(const float* pxlane, uint32_t refine, uint32_t re
     constexpr int abits = SWAP ? 2 : (MODE == 4 ? 3 : 2);
     constexpr int aepbits = MODE == 4 ? 6 : 8;
     const int swap = SWAP;
-    BlkRot<CH4> cb{pxlane, rot < 3 ? rot : -1};
+    const BlkRot<CH4> cb(pxlane, rot < 3 ? rot : -1);
     float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     block_segment<3, true, true>(cb, 0xFFFFu, ep);
     // quantise + index fit, then `refine` times: endpoint fit, quantise +

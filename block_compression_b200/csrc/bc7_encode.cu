@@ -367,6 +367,11 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Wo
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    if (!CH4) {
+        // 3-channel settings: the rotated-out channel reads 255 (BlkRot)
+        __syncthreads();
+        for (int t = threadIdx.x; t < 16 * NB; t += NW * 32) px[48 + t / NB][t % NB] = 255.0f;
+    }
     __syncthreads();
     const int r = blockIdx.y * NW + warp;  // rotation index
     if (r >= P.n45_5) return;              // n45_5 = number of rotations
