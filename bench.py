@@ -57,19 +57,72 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and clock-event reasons of this rank's GPU during the timed
+    region. NVML, sampled every 2 ms on a thread and once more at the start
+    and at the end (so a region shorter than the interval still has
+    samples), the GPU found by its PCI address (NVML numbers every GPU of
+    the machine, not the visible ones); `nvidia-smi -lms 100` by UUID as the
+    fallback."""
+
+    REASON_BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+                   "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.nv = None
+        self.h = None
+        self.samples = []
+        self.max_mhz = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.index)
+        for fmt in ("%08X:%02X:%02X.0", "%04X:%02X:%02X.0"):
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(
+                    (fmt % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)).encode())
+            except pynvml.NVMLError:
+                continue
+        raise RuntimeError("no NVML device at the GPU's PCI address")
+
+    def _sample(self):
+        sm = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+        reasons = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        self.samples.append((float(sm), int(reasons)))
+
+    def _loop(self):
+        while not self.stop.wait(0.002):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        try:
+            self.nv, self.h = self._nvml_handle()
+            self.max_mhz = float(self.nv.nvmlDeviceGetMaxClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            self._sample()
+            self.stop = threading.Event()
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.h = None
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+            sel = str(self.index)
+            try:
+                import torch
+                sel = "GPU-" + str(torch.cuda.get_device_properties(self.index).uuid)
+            except Exception:
+                pass
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", sel, "--query-gpu=" + q,
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -83,6 +136,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.h is not None:
+            self.stop.set()
+            self.t.join(timeout=5)
+            try:
+                self._sample()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -91,6 +151,11 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.samples:
+            sm = [x for x, _ in self.samples]
+            reasons = sorted(n for n, bit in self.REASON_BITS.items() if any(r & bit for _, r in self.samples))
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "nvml"}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -106,7 +171,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def _dist():

@@ -109,6 +109,8 @@ int capture(bc_batch* b) {
         cudaGraphExecDestroy(b->exec);
         b->exec = nullptr;
     }
+    // the BC7 pipeline's side streams must exist before capture begins
+    BATCH_CUDA(bc7_side_streams_init());
     cudaStream_t cs;
     BATCH_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;

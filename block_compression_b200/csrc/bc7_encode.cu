@@ -543,7 +543,12 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaError_t e = cudaStreamIsCapturing(s, &cs);
         if (e != cudaSuccess) return e;
-        if (cs == cudaStreamCaptureStatusNone) {
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        // while `s` captures a graph the side streams join the capture
+        // through the fork event, but are not created then
+        // (bc7_side_streams_init() makes them beforehand)
+        if (cs == cudaStreamCaptureStatusNone || t_side.device == dev) {
             if ((e = t_side.get()) != cudaSuccess) return e;
             if ((e = cudaEventRecord(t_side.fork, s)) != cudaSuccess) return e;
             if ((e = cudaStreamWaitEvent(t_side.st, t_side.fork, 0)) != cudaSuccess) return e;
@@ -632,6 +637,8 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
     return run_pipeline(w, (n + NB - 1) / NB, scratch, 8, s, side_stream);
 }
 
+cudaError_t bc7_side_streams_init() { return bc7::t_side.get(); }
+
 cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
                              const BC7SettingsDev& settings, void* scratch, int search_warps, cudaStream_t s) {
     using namespace bc7;
@@ -641,7 +648,7 @@ cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_tas
     w.tasks = tasks_dev;
     w.tile_task = tile_task_dev;
     w.S = settings;
-    return run_pipeline(w, ntiles, scratch, search_warps, s, false);
+    return run_pipeline(w, ntiles, scratch, search_warps, s, true);
 }
 
 }  // namespace bcn

@@ -47,9 +47,10 @@ void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_
 // BC7 runs as a short pipeline of kernels that exchange per-block state
 // through `scratch` (device memory of at least bc7_scratch_bytes()).
 size_t bc7_scratch_bytes(uint32_t nblocks, const BC7SettingsDev& settings);
-// side_stream: run the mode-4/5 and mode-6 candidates on a library-owned
-// second stream forked from `s` and joined before the final selection (not
-// while `s` is capturing a graph).
+// side_stream: run the independent stage chains on library-owned streams
+// forked from `s` and joined before the final selection. While `s` captures
+// a graph this needs bc7_side_streams_init() on the capturing thread first;
+// without it the pipeline stays on `s`.
 cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, uint32_t bh, uint8_t* dst,
                               const BC7SettingsDev& settings, void* scratch, cudaStream_t s,
                               bool side_stream = true);
@@ -57,6 +58,8 @@ cudaError_t launch_bc7_encode(const uint8_t* src, size_t stride, uint32_t bw, ui
 // (tasks_dev / tile_task_dev in device memory). search_warps: 4 or 8
 // candidates per CTA in the search launches.
 size_t bc7_scratch_bytes_tiles(uint32_t ntiles, const BC7SettingsDev& settings);
+// Creates the calling thread's BC7 side streams for the current device.
+cudaError_t bc7_side_streams_init();
 cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
                              const BC7SettingsDev& settings, void* scratch, int search_warps, cudaStream_t s);
 // Persistent work-queue kernel over the tiles of BC1-BC5 regions: CTAs claim
