@@ -575,7 +575,10 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
     }
     auto search = [&](int mi, cudaStream_t st) {
         const int mode = mi == 0 ? 0 : (mi == 1 ? 2 : (mi == 2 ? 1 : (mi == 3 ? 3 : 7)));
-        if (search_warps == 4) {
+        // 4 candidates per CTA when 8 would leave a last group at most half
+        // full (e.g. 12 candidates: 3 full CTAs of 4 instead of 8 + 4)
+        const int rem = P.count[mi] % 8;
+        if (search_warps == 4 || (rem != 0 && rem <= 4)) {
             dim3 g(ntiles, groups(P.count[mi], 4));
             switch (mode) {
                 case 0: bc7_search_kernel<0, 4><<<g, 128, 0, st>>>(w); break;
