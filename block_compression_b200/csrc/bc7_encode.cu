@@ -21,7 +21,8 @@
 //            per-mode results -> one 128-bit store per block
 //
 // mode4/5 + mode6, search/refine of modes 0/2, and prep -> search/refine of
-// modes 1/3/7 are independent chains, run on three streams.
+// modes 1/3/7 are independent chains, run on their own streams (the refines
+// of modes 1/3/7 on a fourth one).
 //
 // Blocks are staged in shared memory as planar f32 with 128-bit coalesced
 // loads. Every per-candidate computation keeps the reference's operation
@@ -473,19 +474,19 @@ namespace bc7 {
 
 // Carves the scratch arrays out of `scratch` and enqueues the pipeline over
 // `ntiles` tiles.
-// The second and third streams of run_pipeline, with their fork and join
+// The side streams of run_pipeline, with their fork, join and per-search
 // events; per thread and device, created on first use.
 struct SideStream {
-    cudaStream_t st = nullptr, st2 = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
+    cudaStream_t st = nullptr, st2 = nullptr, st3 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr, join3 = nullptr, searched[3] = {};
     int device = -1;
     void release() {
-        for (cudaEvent_t* ev : {&fork, &join, &join2})
+        for (cudaEvent_t* ev : {&fork, &join, &join2, &join3, &searched[0], &searched[1], &searched[2]})
             if (*ev) {
                 cudaEventDestroy(*ev);
                 *ev = nullptr;
             }
-        for (cudaStream_t* q : {&st, &st2})
+        for (cudaStream_t* q : {&st, &st2, &st3})
             if (*q) {
                 cudaStreamDestroy(*q);
                 *q = nullptr;
@@ -500,9 +501,9 @@ struct SideStream {
         release();
         // non-blocking: no implicit ordering with the legacy default stream,
         // only the explicit fork / join events
-        for (cudaStream_t* q : {&st, &st2})
+        for (cudaStream_t* q : {&st, &st2, &st3})
             if ((e = cudaStreamCreateWithFlags(q, cudaStreamNonBlocking)) != cudaSuccess) return e;
-        for (cudaEvent_t* ev : {&fork, &join, &join2})
+        for (cudaEvent_t* ev : {&fork, &join, &join2, &join3, &searched[0], &searched[1], &searched[2]})
             if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return e;
         device = dev;
         return cudaSuccess;
@@ -604,17 +605,31 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
     if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
     if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
     bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);
-    for (int mi = 2; mi < 5; mi++)
-        if (P.count[mi]) search(mi, s);
-    if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (P.count[4]) bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, s>>>(w, ntiles);
-    if (s2 != s) {
+    // modes 1/3/7: each refine starts on a fourth stream as soon as its own
+    // search is done, overlapping the next searches (the refine kernels are
+    // latency-bound at 16 warps per SM)
+    const bool split = s2 != s;
+    for (int mi = 2; mi < 5; mi++) {
+        if (!P.count[mi]) continue;
+        search(mi, s);
+        if (split) {
+            cudaError_t e = cudaEventRecord(t_side.searched[mi - 2], s);
+            if (e != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(t_side.st3, t_side.searched[mi - 2], 0)) != cudaSuccess) return e;
+        }
+        cudaStream_t sr = split ? t_side.st3 : s;
+        if (mi == 2) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+        else if (mi == 3) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+        else bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+    }
+    if (split) {
         cudaError_t e = cudaEventRecord(t_side.join, s2);
         if (e != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s, t_side.join, 0)) != cudaSuccess) return e;
         if ((e = cudaEventRecord(t_side.join2, s3)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(s, t_side.join2, 0)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(t_side.join3, t_side.st3)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, t_side.join3, 0)) != cudaSuccess) return e;
     }
     bc7_select_kernel<<<(ntiles + 7) / 8, 256, 0, s>>>(w, ntiles);
     return cudaGetLastError();
