@@ -329,11 +329,13 @@ BCN_DEV int fit_pixel_int(const int* vi, const int* ia, const int* df, float dv,
 // are the same numbers): eb - ea, the sum of its squares, and the decoder's
 // interpolation (64 - w) * ia + w * ib + 32 written as
 // (64 * ia + 32) + w * (ib - ia), which is non-negative, so / 64 is >> 6.
-// INT: pixels and endpoints are 8-bit integers (BC7), so the projection is an
-// integer divided by an integer, both at most 4 * 255^2 in magnitude; it is
-// then computed with the divisor's reciprocal and one fused correction step,
-// which equals the IEEE quotient over that whole domain (checked
-// exhaustively by the oracle test). Otherwise IEEE division (BC6H).
+// INT: pixels and endpoints are 8-bit integers (BC7), so each pixel is
+// fitted in integer arithmetic by fit_pixel_int (the projection is an
+// integer divided by an integer, both at most 4 * 255^2 in magnitude, taken
+// with the divisor's reciprocal and one fused correction step, which equals
+// the IEEE quotient over that whole domain -- checked exhaustively by the
+// oracle test -- and the pixel errors and their total are exact integers).
+// Otherwise the float path with IEEE division (BC6H).
 template <int CH, int BITS, int PAIRS, bool INT = false, class B>
 BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
     if (INT) {
