@@ -40,7 +40,7 @@
 
 // Minimum resident CTAs per SM requested from the register allocator.
 #ifndef BCN_MODE45_MINB
-#define BCN_MODE45_MINB 6
+#define BCN_MODE45_MINB 7
 #endif
 #ifndef BCN_REFINE_MINB
 #define BCN_REFINE_MINB 4
