@@ -192,6 +192,21 @@ def max_over_ranks(ms, pg, device):
     return float(t.item())
 
 
+def bc7_kernel_count(s):
+    """Kernels one BC7 encode launches (bc7_encode.cu run_pipeline): prep, a
+    search and a refine per mode with candidates (0, 2, 1, 3, 7), the three
+    mode-4/5 launches when rotations are searched, mode 6, select."""
+    ms = [bool(x) for x in s.mode_selection]
+    run13 = ms[1] and bool(s.fast_skip_threshold_mode1 or s.fast_skip_threshold_mode3)
+    run7 = ms[1] and bool(s.fast_skip_threshold_mode7)
+    counts = [16 if ms[0] else 0, 64 if (ms[0] and not s.skip_mode2) else 0,
+              s.fast_skip_threshold_mode1 if run13 else 0, s.fast_skip_threshold_mode3 if run13 else 0,
+              s.fast_skip_threshold_mode7 if run7 else 0]
+    nsearch = sum(1 for c in counts if c)
+    nrot = max(0, int(s.channels) - int(s.mode45_channel0)) if ms[2] else 0
+    return 1 + 2 * nsearch + (3 if nrot else 0) + (1 if ms[3] else 0) + 1
+
+
 def job_mpx_s(world, px_per_rank_step, steps, ms):
     """Whole-job throughput of a weak-scaling run: every rank encodes
     px_per_rank_step pixels per step; ms is the max-over-ranks time."""
@@ -399,7 +414,9 @@ def gpu_bench(args, world, rank, local):
             "config": {"workload": WORKLOAD, "px_per_step": px_per_step, "l2": "flushed (256 MiB write) before each step",
                        "bc7_settings": "alpha_basic"},
             "e2e": {"value": e2e_value, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": len(jobs) * args.steps,
+            # our kernels in the timed region: the BC7 pipeline plus one
+            # kernel each for BC3, BC4 and BC5, per step
+            "gpu_launches": (bc7_kernel_count(s7) + len(jobs) - 1) * args.steps,
             "per_variant_mpx_s": per_variant,
             "roofline": roof, "roofline_hbm_path": hbm,
             "cpu_baseline": cpu,

@@ -1,6 +1,7 @@
-"""The bench's clock record: throttle reasons from NVML's clock-event bit
-mask, the median SM clock, and the nvidia-smi CSV fallback. A fake NVML
-module stands in for the GPU (nothing here touches a device)."""
+"""Host logic of the bench line: the clock record (throttle reasons from
+NVML's clock-event bit mask, the median SM clock, the nvidia-smi CSV
+fallback; a fake NVML stands in for the GPU) and the count of our kernels
+per step."""
 import os
 import sys
 import types
@@ -42,3 +43,13 @@ def test_nvidia_smi_lines_are_the_fallback():
     s = c.summary()
     assert s["source"] == "nvidia-smi" and s["samples"] == 2
     assert s["sm_mhz"] == 1957.5 and s["sm_max_mhz"] == 1965.0 and s["reasons"] == ["sw_power_cap"]
+
+
+def test_bc7_kernel_count_matches_the_pipeline():
+    from block_compression_b200.settings import BC7Settings
+    # alpha_basic: prep, searches and refines of modes 0, 1, 3 and 7 (mode 2
+    # skipped), three mode-4/5 launches, mode 6, select -- the 14 BC7 kernels
+    # of the benchmark's launch list
+    assert bench.bc7_kernel_count(BC7Settings.alpha_basic()) == 14
+    # opaque_basic: no mode 7 candidates
+    assert bench.bc7_kernel_count(BC7Settings.opaque_basic()) == 12
