@@ -56,6 +56,16 @@ def _load():
         "bc_decompress_blocks_as_rgba16f": ([I, U32, U32, P, S, P, S], I),
         "bc_decompress_blocks_as_rgba32f": ([I, U32, U32, P, S, P, S], I),
         "bc_decompress_device": ([I, U32, U32, P, S, P, S, I, P], I),
+        "bc_decode_block_min_len": ([I, S], S),
+        "bc_decode_block_bc1": ([P, S, P, S, S], I),
+        "bc_decode_block_bc2": ([P, S, P, S, S], I),
+        "bc_decode_block_bc3": ([P, S, P, S, S], I),
+        "bc_decode_block_bc4": ([P, S, P, S, S], I),
+        "bc_decode_block_bc5": ([P, S, P, S, S], I),
+        "bc_decode_block_bc6h": ([P, S, P, S, S, I], I),
+        "bc_decode_block_bc6h_float": ([P, S, P, S, S, I], I),
+        "bc_decode_block_bc7": ([P, S, P, S, S], I),
+        "bc_decode_blocks_device": ([I, I, P, S, P, S, S, S, P], I),
         "bc_compressor_create": ([I, ctypes.POINTER(P)], I),
         "bc_compressor_destroy": ([P], I),
         "bc_compressor_add_task": ([P, I, P, P, S, S, U32, U32, U32, P, S, U32], I),

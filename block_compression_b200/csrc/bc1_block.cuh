@@ -1,7 +1,8 @@
-// BC1 colour-block primitives shared by the BC1-BC5 kernels (bc15.cu) and
-// the endpoint-refinement kernels (refine.cu): the RGB565 conversions of the
-// encoder (src/encode/bc1_to_5.rs:258-278) and the bit-exact colour-block
-// decoder (src/decode/block.rs:124-197).
+// BC1-BC5 block primitives shared by the BC1-BC5 kernels (bc15.cu), the
+// per-block decoders (bc_decode.cu) and the endpoint-refinement kernels
+// (refine.cu): the RGB565 conversions of the encoder
+// (src/encode/bc1_to_5.rs:258-278) and the bit-exact colour-block and
+// smooth-alpha decoders (src/decode/block.rs:124-258).
 #pragma once
 #include "bc_common.cuh"
 
@@ -42,6 +43,28 @@ BCN_DEV void decode_color(uint32_t c01, uint32_t idx, bool opaque, uint32_t out[
     }
 #pragma unroll
     for (int k = 0; k < 16; k++) out[k] = ref[(idx >> (2 * k)) & 3];
+}
+
+// block.rs:221-258. The 8-entry palette is kept as 8 bytes in two registers
+// and indexed with a byte permute (no local-memory array).
+BCN_DEV void decode_smooth(uint32_t lo, uint32_t hi, uint32_t out[16]) {
+    uint32_t a0 = lo & 0xFF, a1 = (lo >> 8) & 0xFF;
+    uint32_t p_lo, p_hi;
+    if (a0 > a1) {
+        p_lo = a0 | (a1 << 8) | (((6 * a0 + a1) / 7) << 16) | (((5 * a0 + 2 * a1) / 7) << 24);
+        p_hi = ((4 * a0 + 3 * a1) / 7) | (((3 * a0 + 4 * a1) / 7) << 8) | (((2 * a0 + 5 * a1) / 7) << 16) |
+               (((a0 + 6 * a1) / 7) << 24);
+    } else {
+        p_lo = a0 | (a1 << 8) | (((4 * a0 + a1) / 5) << 16) | (((3 * a0 + 2 * a1) / 5) << 24);
+        p_hi = ((2 * a0 + 3 * a1) / 5) | (((a0 + 4 * a1) / 5) << 8) | (0u << 16) | (255u << 24);
+    }
+    // 48 index bits: pixels 0-7 in the low 24, pixels 8-15 in the high 24
+    uint32_t i0 = (lo >> 16) | ((hi & 0xFF) << 16), i1 = hi >> 8;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        uint32_t sel = ((k < 8 ? i0 : i1) >> (3 * (k & 7))) & 7u;
+        out[k] = __byte_perm(p_lo, p_hi, sel) & 0xFFu;
+    }
 }
 
 }  // namespace bcn

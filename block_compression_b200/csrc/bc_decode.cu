@@ -174,8 +174,30 @@ BCN_DEV int unquantize_u(int v, int bits) {
     return ((v << 16) + 0x8000) >> bits;
 }
 
-// Unsigned BC6H (the only form the image drivers use): 16 pixels of RGB
-// f16 bit patterns.
+// block.rs:1288-1306, the signed branch of unquantize.
+BCN_DEV int unquantize_s(int v, int bits) {
+    if (bits >= 16) return v;
+    const bool neg = v < 0;
+    const int m = neg ? -v : v;
+    int u;
+    if (m == 0) u = 0;
+    else if (m >= (1 << (bits - 1)) - 1) u = 0x7FFF;
+    else u = ((m << 15) + 0x4000) >> (bits - 1);
+    return neg ? -u : u;
+}
+
+// block.rs:1311-1331: the interpolated value scaled by 31/64 (unsigned) or
+// by 31/32 to a sign-magnitude binary16 (signed).
+template <bool SIGNED>
+BCN_DEV uint32_t finish_unquantize(int v) {
+    if (!SIGNED) return (uint32_t)((v * 31) >> 6) & 0xFFFFu;
+    const int s = v < 0 ? -(((-v) * 31) >> 5) : (v * 31) >> 5;
+    return s < 0 ? (0x8000u | (uint32_t)(-s)) : (uint32_t)s;
+}
+
+// BC6H block decode, signed or unsigned (the image drivers use the unsigned
+// form; the per-block decoders take either): 16 pixels of RGB f16 bit
+// patterns.
 // LSB-first reader over the block at a position the compiler can track: each
 // mode's case sets the start position and reads fixed widths, so every field
 // resolves to a fixed bit offset (funnel shifts, no 128-bit shifting).
@@ -193,7 +215,8 @@ struct PosBits {
 
 // Output: 48 f16 bit patterns (pixel k's RGB at elements 3k..3k+2), packed
 // two per word: element e in bits 16 * (e & 1) of out[e >> 1].
-BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint32_t out[24]) {
+template <bool SIGNED>
+BCN_DEV void decode_bc6h_block(uint64_t lo, uint64_t hi, uint32_t out[24]) {
     const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
     PosBits bs{d, 0};
     int r[4] = {0, 0, 0, 0}, g[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
@@ -348,15 +371,31 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint32_t out[24]) {
     const int br = tab14(0x0506050404050605ULL, 0x0408090A0605ULL);
     const int bgb = tab14(0x0605050405040605ULL, 0x0408090A0605ULL);
     const int bbb = tab14(0x0505050504040605ULL, 0x0408090A0606ULL);
-    if (mode != 9 && mode != 10) {
+    if (SIGNED) {  // block.rs:698-702
+        r[0] = extend_sign(r[0], bits0);
+        g[0] = extend_sign(g[0], bits0);
+        b[0] = extend_sign(b[0], bits0);
+    }
+    // block.rs:704-719: the other endpoints are sign-extended deltas from
+    // endpoint 0 (modes 9 and 10 store them directly; the signed form still
+    // sign-extends them), wrapped to the endpoint precision.
+    if ((mode != 9 && mode != 10) || SIGNED) {
+        const bool delta = mode != 9 && mode != 10;
         for (int i = 1; i < (np + 1) * 2; i++) {
             int rr = extend_sign(i == 1 ? r[1] : (i == 2 ? r[2] : r[3]), br);
             int gg = extend_sign(i == 1 ? g[1] : (i == 2 ? g[2] : g[3]), bgb);
             int bb = extend_sign(i == 1 ? b[1] : (i == 2 ? b[2] : b[3]), bbb);
-            int m = (1 << bits0) - 1;
-            rr = (rr + r[0]) & m;
-            gg = (gg + g[0]) & m;
-            bb = (bb + b[0]) & m;
+            if (delta) {
+                int m = (1 << bits0) - 1;
+                rr = (rr + r[0]) & m;
+                gg = (gg + g[0]) & m;
+                bb = (bb + b[0]) & m;
+                if (SIGNED) {
+                    rr = extend_sign(rr, bits0);
+                    gg = extend_sign(gg, bits0);
+                    bb = extend_sign(bb, bits0);
+                }
+            }
             if (i == 1) { r[1] = rr; g[1] = gg; b[1] = bb; }
             else if (i == 2) { r[2] = rr; g[2] = gg; b[2] = bb; }
             else { r[3] = rr; g[3] = gg; b[3] = bb; }
@@ -365,9 +404,9 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint32_t out[24]) {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         if (i >= (np + 1) * 2) break;
-        r[i] = unquantize_u(r[i], bits0);
-        g[i] = unquantize_u(g[i], bits0);
-        b[i] = unquantize_u(b[i], bits0);
+        r[i] = SIGNED ? unquantize_s(r[i], bits0) : unquantize_u(r[i], bits0);
+        g[i] = SIGNED ? unquantize_s(g[i], bits0) : unquantize_u(g[i], bits0);
+        b[i] = SIGNED ? unquantize_s(b[i], bits0) : unquantize_u(b[i], bits0);
     }
     // Index bits: 46 bits from bit 82 (two subsets, 3-bit indices) or 63 bits
     // from bit 65 (one subset, 4-bit); a zero is re-inserted above each anchor
@@ -391,8 +430,9 @@ BCN_DEV void decode_bc6h_block_u(uint64_t lo, uint64_t hi, uint32_t out[24]) {
         int r0 = e ? r[2] : r[0], r1 = e ? r[3] : r[1];
         int g0 = e ? g[2] : g[0], g1 = e ? g[3] : g[1];
         int b0 = e ? b[2] : b[0], b1 = e ? b[3] : b[1];
-        const uint32_t c[3] = {(uint32_t)((interp(r0, r1, w) * 31) >> 6), (uint32_t)((interp(g0, g1, w) * 31) >> 6),
-                               (uint32_t)((interp(b0, b1, w) * 31) >> 6)};
+        const uint32_t c[3] = {finish_unquantize<SIGNED>(interp(r0, r1, w)),
+                               finish_unquantize<SIGNED>(interp(g0, g1, w)),
+                               finish_unquantize<SIGNED>(interp(b0, b1, w))};
 #pragma unroll
         for (int ch = 0; ch < 3; ch++) {
             const int e = k * 3 + ch;
@@ -472,7 +512,7 @@ __global__ void __launch_bounds__(kSortCta) bc6h_decode_sorted_kernel(const uint
             uint32_t i = base + t;
             if (i < n) {
                 uint32_t h[24];
-                decode_bc6h_block_u((uint64_t)v.x | ((uint64_t)v.y << 32), (uint64_t)v.z | ((uint64_t)v.w << 32), h);
+                decode_bc6h_block<false>((uint64_t)v.x | ((uint64_t)v.y << 32), (uint64_t)v.z | ((uint64_t)v.w << 32), h);
                 uint32_t by = i / bw, bx = i - by * bw;
 #pragma unroll
                 for (int y = 0; y < 4; y++)
@@ -488,7 +528,7 @@ __global__ void __launch_bounds__(kSortCta) bc6h_decode_sorted_kernel(const uint
         uint4 b = s_blk[t];
         uint32_t o = s_orig[t];
         uint32_t h[24];
-        decode_bc6h_block_u((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), h);
+        decode_bc6h_block<false>((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), h);
 #pragma unroll
         for (int q = 0; q < 24; q++) s_out[q * kSortCta + o] = h[q];
         __syncthreads();
@@ -518,7 +558,7 @@ __global__ void __launch_bounds__(128) bc6h_decode_kernel(const uint8_t* __restr
         for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
         for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
         uint32_t h[24];
-        decode_bc6h_block_u(lo, hi, h);
+        decode_bc6h_block<false>(lo, hi, h);
         for (int y = 0; y < 4; y++) {
             size_t row = (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
             for (int x = 0; x < 4; x++) {
@@ -574,4 +614,126 @@ namespace bcn {
 cudaError_t set_half_to_srgb_table(const uint8_t* host) {
     return cudaMemcpyToSymbol(g_half_to_srgb, host, sizeof(g_half_to_srgb));
 }
+}  // namespace bcn
+
+// ---- per-block decoders (src/decode/block.rs:50-119, 262, 774, 801) ------------
+//
+// The reference's per-block functions write one block's texels at a caller
+// pitch, element by element; with a pitch shorter than a decoded row the rows
+// overlap and later writes win. One thread decodes one block and issues its
+// writes in the reference's order (row, pixel, channel; BC2/BC3 colour before
+// alpha, BC5 red before green), so the final contents match for every pitch.
+// Blocks of one launch write to disjoint ranges (block i starts at element
+// i * out_block_stride).
+#include "bc1_block.cuh"
+
+namespace bcn {
+
+// Loads `n` (8 or 16) bytes of block i as little-endian words.
+BCN_DEV void load_block_words(const uint8_t* __restrict__ blocks, size_t i, int n, uint32_t w[4]) {
+    const uint8_t* b = blocks + i * (size_t)n;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        w[q] = 0;
+        if (q * 4 < n)
+            for (int j = 0; j < 4; j++) w[q] |= (uint32_t)b[q * 4 + j] << (8 * j);
+    }
+}
+
+// RGBA8 texels as 4-byte groups at i * pitch + j * 4 (decode_color_block,
+// BC7): the colour pass.
+BCN_DEV void write_rgba_pass(uint8_t* o, size_t pitch, const uint32_t px[16]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            for (int c = 0; c < 4; c++) o[i * pitch + j * 4 + c] = (uint8_t)(px[i * 4 + j] >> (8 * c));
+}
+
+// One byte per texel at i * pitch + j * step (the alpha / single-channel passes).
+BCN_DEV void write_byte_pass(uint8_t* o, size_t pitch, int step, const uint32_t v[16]) {
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) o[i * pitch + j * step] = (uint8_t)v[i * 4 + j];
+}
+
+__global__ void __launch_bounds__(128) decode_blocks_kernel(int kind, const uint8_t* __restrict__ blocks,
+                                                            size_t nblocks, void* out, size_t pitch,
+                                                            size_t out_block_stride) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nblocks;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int nbytes = (kind == BLOCK_BC1 || kind == BLOCK_BC4) ? 8 : 16;
+        uint32_t w[4];
+        load_block_words(blocks, i, nbytes, w);
+        const size_t base = i * out_block_stride;
+        uint32_t px[16], a[16];
+        switch (kind) {
+            case BLOCK_BC1: {  // block.rs:50-57
+                uint8_t* o = reinterpret_cast<uint8_t*>(out) + base;
+                decode_color(w[0], w[1], false, px);
+                write_rgba_pass(o, pitch, px);
+                break;
+            }
+            case BLOCK_BC2: {  // block.rs:61-72: colour of bytes 8..16, then the 4-bit alpha
+                uint8_t* o = reinterpret_cast<uint8_t*>(out) + base;
+                decode_color(w[2], w[3], true, px);
+                write_rgba_pass(o, pitch, px);
+                for (int k = 0; k < 16; k++) a[k] = (((k < 8 ? w[0] : w[1]) >> (4 * (k & 7))) & 15u) * 17u;
+                write_byte_pass(o + 3, pitch, 4, a);
+                break;
+            }
+            case BLOCK_BC3: {  // block.rs:76-91
+                uint8_t* o = reinterpret_cast<uint8_t*>(out) + base;
+                decode_color(w[2], w[3], true, px);
+                write_rgba_pass(o, pitch, px);
+                decode_smooth(w[0], w[1], a);
+                write_byte_pass(o + 3, pitch, 4, a);
+                break;
+            }
+            case BLOCK_BC4: {  // block.rs:95-102
+                decode_smooth(w[0], w[1], a);
+                write_byte_pass(reinterpret_cast<uint8_t*>(out) + base, pitch, 1, a);
+                break;
+            }
+            case BLOCK_BC5: {  // block.rs:106-119
+                uint8_t* o = reinterpret_cast<uint8_t*>(out) + base;
+                decode_smooth(w[0], w[1], a);
+                write_byte_pass(o, pitch, 2, a);
+                decode_smooth(w[2], w[3], a);
+                write_byte_pass(o + 1, pitch, 2, a);
+                break;
+            }
+            case BLOCK_BC7: {  // block.rs:801-1252
+                decode_bc7_block((uint64_t)w[0] | ((uint64_t)w[1] << 32), (uint64_t)w[2] | ((uint64_t)w[3] << 32),
+                                 px);
+                write_rgba_pass(reinterpret_cast<uint8_t*>(out) + base, pitch, px);
+                break;
+            }
+            default: {  // BC6H: half (block.rs:262-769) or float (:774-796), unsigned or signed
+                const uint64_t lo = (uint64_t)w[0] | ((uint64_t)w[1] << 32), hi = (uint64_t)w[2] | ((uint64_t)w[3] << 32);
+                uint32_t h[24];
+                const bool is_signed = kind == BLOCK_BC6H_HALF_SIGNED || kind == BLOCK_BC6H_FLOAT_SIGNED;
+                if (is_signed) decode_bc6h_block<true>(lo, hi, h);
+                else decode_bc6h_block<false>(lo, hi, h);
+                const bool as_float = kind == BLOCK_BC6H_FLOAT || kind == BLOCK_BC6H_FLOAT_SIGNED;
+                for (int i2 = 0; i2 < 4; i2++)
+                    for (int j = 0; j < 4; j++)
+                        for (int c = 0; c < 3; c++) {
+                            const int e = (i2 * 4 + j) * 3 + c;
+                            const uint16_t v = (uint16_t)(h[e >> 1] >> (16 * (e & 1)));
+                            const size_t at = base + i2 * pitch + j * 3 + c;
+                            if (as_float) reinterpret_cast<float*>(out)[at] = __half2float(__ushort_as_half(v));
+                            else reinterpret_cast<uint16_t*>(out)[at] = v;
+                        }
+                break;
+            }
+        }
+    }
+}
+
+void launch_decode_blocks(int kind, const uint8_t* blocks, size_t nblocks, void* out, size_t pitch,
+                          size_t out_block_stride, cudaStream_t s) {
+    if (nblocks == 0) return;
+    size_t g = (nblocks + 127) / 128;
+    if (g > 148u * 64u) g = 148u * 64u;
+    decode_blocks_kernel<<<(unsigned)g, 128, 0, s>>>(kind, blocks, nblocks, out, pitch, out_block_stride);
+}
+
 }  // namespace bcn

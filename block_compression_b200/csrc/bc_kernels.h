@@ -76,6 +76,19 @@ void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format,
 void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
                         cudaStream_t s);
 
+// Per-block decoders (the reference's decode_block_* functions): kinds in
+// the order of the public BC_BLOCK_* values, plus the signed BC6H forms.
+enum BlockKind {
+    BLOCK_BC1 = 0, BLOCK_BC2 = 1, BLOCK_BC3 = 2, BLOCK_BC4 = 3, BLOCK_BC5 = 4,
+    BLOCK_BC6H_HALF = 5, BLOCK_BC6H_FLOAT = 6, BLOCK_BC7 = 7,
+    BLOCK_BC6H_HALF_SIGNED = 8, BLOCK_BC6H_FLOAT_SIGNED = 9
+};
+// Block i (8 or 16 bytes at blocks + i * size) decoded to `out` starting at
+// element i * out_block_stride, rows `pitch` elements apart, written in the
+// reference's element order.
+void launch_decode_blocks(int kind, const uint8_t* blocks, size_t nblocks, void* out, size_t pitch,
+                          size_t out_block_stride, cudaStream_t s);
+
 // Settings check shared by every BC7 entry point (BC_OK or a BC_ERR_* code),
 // and the per-thread record behind bc_last_cuda_error().
 int validate_bc7_settings(const void* settings);

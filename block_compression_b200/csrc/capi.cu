@@ -552,6 +552,127 @@ extern "C" int bc_decompress_blocks_as_rgba32f(int variant, uint32_t width, uint
     return host_decode(variant, width, height, blocks, blocks_len, rgba, rgba_len, 2);
 }
 
+// ---- per-block decoders (src/decode/block.rs:50-119, 262, 774, 801) --------------------------
+
+// Bytes one compressed block of `kind` occupies, and the element size of its output.
+static size_t block_kind_bytes(int kind) { return (kind == BC_BLOCK_BC1 || kind == BC_BLOCK_BC4) ? 8 : 16; }
+static size_t block_kind_elem(int kind) {
+    return kind == BC_BLOCK_BC6H ? 2 : (kind == BC_BLOCK_BC6H_FLOAT ? 4 : 1);
+}
+
+// Output elements the reference's slice indexing needs (it panics on
+// less): one past the last element written, and for the BC6H float form also
+// 4 * pitch, because it advances its output slice by the pitch after each of
+// the 4 rows (block.rs:789-795).
+extern "C" size_t bc_decode_block_min_len(int kind, size_t pitch) {
+    switch (kind) {
+        case BC_BLOCK_BC1: case BC_BLOCK_BC2: case BC_BLOCK_BC3: case BC_BLOCK_BC7: return 3 * pitch + 16;
+        case BC_BLOCK_BC4: return 3 * pitch + 4;
+        case BC_BLOCK_BC5: return 3 * pitch + 8;
+        case BC_BLOCK_BC6H: return 3 * pitch + 12;
+        case BC_BLOCK_BC6H_FLOAT: return 4 * pitch > 3 * pitch + 12 ? 4 * pitch : 3 * pitch + 12;
+        default: return 0;
+    }
+}
+
+static int internal_block_kind(int kind, int is_signed) {
+    if (kind == BC_BLOCK_BC6H) return is_signed ? BLOCK_BC6H_HALF_SIGNED : BLOCK_BC6H_HALF;
+    if (kind == BC_BLOCK_BC6H_FLOAT) return is_signed ? BLOCK_BC6H_FLOAT_SIGNED : BLOCK_BC6H_FLOAT;
+    return kind;
+}
+
+static int check_block_decode(int kind, int is_signed, size_t nblocks, size_t out_len, size_t pitch,
+                              size_t out_block_stride) {
+    if (kind < BC_BLOCK_BC1 || kind > BC_BLOCK_BC7) return BC_ERR_VARIANT;
+    if (is_signed && kind != BC_BLOCK_BC6H && kind != BC_BLOCK_BC6H_FLOAT) return BC_ERR_VARIANT;
+    if (nblocks == 0) return BC_OK;
+    const size_t need = bc_decode_block_min_len(kind, pitch);
+    if (nblocks > 1 && out_block_stride > (SIZE_MAX - need) / (nblocks - 1)) return BC_ERR_DST_SIZE;
+    if (out_len < (nblocks - 1) * out_block_stride + need) return BC_ERR_DST_SIZE;
+    return BC_OK;
+}
+
+extern "C" int bc_decode_blocks_device(int kind, int is_signed, const uint8_t* blocks_dev, size_t nblocks,
+                                       void* out_dev, size_t out_len, size_t pitch, size_t out_block_stride,
+                                       void* stream) {
+    int rc = check_block_decode(kind, is_signed, nblocks, out_len, pitch, out_block_stride);
+    if (rc != BC_OK || nblocks == 0) return rc;
+    if (!blocks_dev || !out_dev) return BC_ERR_NULL;
+    launch_decode_blocks(internal_block_kind(kind, is_signed), blocks_dev, nblocks, out_dev, pitch,
+                         out_block_stride, (cudaStream_t)stream);
+    BC_CUDA(cudaGetLastError());
+    return BC_OK;
+}
+
+// One block from host memory: staged through the device (the output's
+// current contents are carried through, since the reference leaves every
+// element it does not write untouched), decoded, copied back; synchronous.
+static int host_decode_block(int kind, int is_signed, const uint8_t* compressed, size_t compressed_len, void* out,
+                             size_t out_len, size_t pitch) {
+    int rc = check_block_decode(kind, is_signed, 1, out_len, pitch, 0);
+    if (rc != BC_OK) return rc;
+    if (!compressed || !out) return BC_ERR_NULL;
+    const size_t nb = block_kind_bytes(kind);
+    if (compressed_len < nb) return BC_ERR_SRC_SIZE;
+    const size_t bytes = bc_decode_block_min_len(kind, pitch) * block_kind_elem(kind);
+    void *dsrc = nullptr, *ddst = nullptr;
+    rc = t_staging.get(0, nb, &dsrc);
+    if (rc != BC_OK) return rc;
+    rc = t_staging.get(1, bytes, &ddst);
+    if (rc != BC_OK) return rc;
+    cudaStream_t s = 0;
+    BC_CUDA(cudaMemcpyAsync(dsrc, compressed, nb, cudaMemcpyHostToDevice, s));
+    BC_CUDA(cudaMemcpyAsync(ddst, out, bytes, cudaMemcpyHostToDevice, s));
+    launch_decode_blocks(internal_block_kind(kind, is_signed), (const uint8_t*)dsrc, 1, ddst, pitch, 0, s);
+    BC_CUDA(cudaGetLastError());
+    BC_CUDA(cudaMemcpyAsync(out, ddst, bytes, cudaMemcpyDeviceToHost, s));
+    BC_CUDA(cudaStreamSynchronize(s));
+    return BC_OK;
+}
+
+extern "C" int bc_decode_block_bc1(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC1, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+extern "C" int bc_decode_block_bc2(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC2, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+extern "C" int bc_decode_block_bc3(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC3, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+extern "C" int bc_decode_block_bc4(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC4, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+extern "C" int bc_decode_block_bc5(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC5, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+extern "C" int bc_decode_block_bc6h(const uint8_t* compressed_block, size_t compressed_len,
+                                    uint16_t* decompressed_block, size_t decompressed_len, size_t destination_pitch,
+                                    int is_signed) {
+    return host_decode_block(BC_BLOCK_BC6H, is_signed, compressed_block, compressed_len, decompressed_block,
+                             decompressed_len, destination_pitch);
+}
+extern "C" int bc_decode_block_bc6h_float(const uint8_t* compressed_block, size_t compressed_len,
+                                          float* decompressed_block, size_t decompressed_len, size_t destination_pitch,
+                                          int is_signed) {
+    return host_decode_block(BC_BLOCK_BC6H_FLOAT, is_signed, compressed_block, compressed_len, decompressed_block,
+                             decompressed_len, destination_pitch);
+}
+extern "C" int bc_decode_block_bc7(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                                   size_t decompressed_len, size_t destination_pitch) {
+    return host_decode_block(BC_BLOCK_BC7, 0, compressed_block, compressed_len, decompressed_block, decompressed_len,
+                             destination_pitch);
+}
+
 // ---- task queue (src/block_compressor.rs:44-590) --------------------------------------------
 
 struct BcTask {

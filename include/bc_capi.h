@@ -4,7 +4,7 @@
  * block_compression v0.3.0 (novacrazy/block_compression). Every entry point
  * below names the reference interface it replaces. A Rust shim binds these
  * symbols with `extern "C"` and turns a negative status into the same panic
- * the reference raises (INTEGRATION.md shows the binding).
+ * the reference raises.
  *
  * Conventions
  *   - Every function returns an int status: BC_OK (0) or a negative BC_ERR_*.
@@ -163,6 +163,56 @@ int bc_decompress_blocks_as_rgba32f(int variant, uint32_t width, uint32_t height
 int bc_decompress_device(int variant, uint32_t width, uint32_t height, const uint8_t* blocks_dev,
                          size_t blocks_len, void* out_dev, size_t out_len, int out_format,
                          void* stream);
+
+/* ---- per-block decoders ----------------------------------------------------
+ * decode::decode_block_bc1 .. decode_block_bc5 (src/decode/block.rs:50-119),
+ * decode_block_bc6h (:262), decode_block_bc6h_float (:774) and
+ * decode_block_bc7 (:801), re-exported by src/decode.rs:7-16. One block of
+ * 8 (BC1, BC4) or 16 bytes is decoded into `decompressed_block` with
+ * `destination_pitch` output elements between rows (bytes for BC1-BC5 and
+ * BC7: RGBA8, R8 for BC4, RG8 for BC5; binary16 values for bc6h; floats for
+ * bc6h_float), exactly as the reference writes it:
+ *  - only the elements the reference writes are written (e.g. every 4th byte
+ *    for BC4 at pitch 4 is not: BC4 writes 1 byte per texel), and in its
+ *    order, so pitches shorter than a decoded row (overlapping rows) give the
+ *    reference's contents too;
+ *  - BC6H outputs RGB triplets; is_signed selects the signed-format decode;
+ *  - decompressed_len (in elements) must be at least
+ *    bc_decode_block_min_len(kind, pitch), where the reference's slice
+ *    indexing would panic (BC_ERR_DST_SIZE); compressed_len must cover the
+ *    block (BC_ERR_SRC_SIZE).
+ * Host buffers, synchronous (the block is staged through the current device). */
+#define BC_BLOCK_BC1 0
+#define BC_BLOCK_BC2 1
+#define BC_BLOCK_BC3 2
+#define BC_BLOCK_BC4 3
+#define BC_BLOCK_BC5 4
+#define BC_BLOCK_BC6H 5       /* binary16 output (decode_block_bc6h) */
+#define BC_BLOCK_BC6H_FLOAT 6 /* f32 output (decode_block_bc6h_float) */
+#define BC_BLOCK_BC7 7
+size_t bc_decode_block_min_len(int kind, size_t destination_pitch);
+int bc_decode_block_bc1(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+int bc_decode_block_bc2(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+int bc_decode_block_bc3(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+int bc_decode_block_bc4(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+int bc_decode_block_bc5(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+int bc_decode_block_bc6h(const uint8_t* compressed_block, size_t compressed_len, uint16_t* decompressed_block,
+                         size_t decompressed_len, size_t destination_pitch, int is_signed);
+int bc_decode_block_bc6h_float(const uint8_t* compressed_block, size_t compressed_len, float* decompressed_block,
+                               size_t decompressed_len, size_t destination_pitch, int is_signed);
+int bc_decode_block_bc7(const uint8_t* compressed_block, size_t compressed_len, uint8_t* decompressed_block,
+                        size_t decompressed_len, size_t destination_pitch);
+/* Device form, stream-ordered: nblocks consecutive blocks of `kind` from
+ * blocks_dev; block i is decoded as above into out_dev starting at element
+ * i * out_block_stride (out_len elements in all). The output ranges of
+ * different blocks must not overlap (their write order is not defined). */
+int bc_decode_blocks_device(int kind, int is_signed, const uint8_t* blocks_dev, size_t nblocks, void* out_dev,
+                            size_t out_len, size_t destination_pitch, size_t out_block_stride, void* stream);
 
 /* ---- GpuBlockCompressor task interface (src/block_compressor.rs:44-590) ---- */
 typedef struct bc_compressor bc_compressor;

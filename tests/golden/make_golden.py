@@ -1,9 +1,9 @@
 """Generates the golden fixtures in this folder from the reference sources.
 
-Run in a checkout that has the reference crate (novacrazy/block_compression
-v0.3.0) available; the path defaults to /root/reference and can be set with
-BCN_REFERENCE_DIR. The fixtures are committed; nothing at test time reads the
-reference tree.
+Run where the reference crate (novacrazy/block_compression v0.3.0) is
+checked out, giving its path as the first argument or in BCN_REFERENCE_DIR:
+`python tests/golden/make_golden.py <reference checkout>`. The fixtures are
+committed; nothing at test time reads the reference tree.
 
 Outputs
   decoder_kat.json      the 18 known-answer tests of src/decode/block.rs:1405-1841
@@ -17,7 +17,7 @@ import re
 import struct
 import sys
 
-REF = os.environ.get("BCN_REFERENCE_DIR", "/root/reference")
+REF = None
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -89,6 +89,10 @@ def presets(settings_rs):
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BCN_REFERENCE_DIR")
+    if not REF:
+        sys.exit("usage: make_golden.py <reference checkout> (or set BCN_REFERENCE_DIR)")
     block_rs = open(os.path.join(REF, "src/decode/block.rs")).read()
     common_rs = open(os.path.join(REF, "src/encode/common.rs")).read()
     settings_rs = open(os.path.join(REF, "src/settings.rs")).read()

@@ -116,3 +116,27 @@ def test_python_api_raises_like_reference_panics(bcn):
         bcn.encode.compress_rgba8(V.BC1, np.zeros(16 * 6 * 4, np.uint8), np.zeros(64, np.uint8), 6, 4, 24)
     with pytest.raises(bcn.BcError):
         bcn.decode.decompress_blocks_as_rgba8(V.BC1, 8, 8, np.zeros(31, np.uint8), np.zeros(256, np.uint8))
+
+
+def test_block_decoder_length_rules_without_gpu(bcn):
+    """The per-block decoders need the output length the reference's slice
+    indexing needs (src/decode/block.rs); shorter buffers, short source blocks
+    and is_signed on a non-BC6H kind are rejected before any CUDA work."""
+    L = bcn.lib
+    assert bcn.decode.block_min_len("bc1", 16) == 64
+    assert bcn.decode.block_min_len("bc7", 8) == 40
+    assert bcn.decode.block_min_len("bc4", 4) == 16
+    assert bcn.decode.block_min_len("bc5", 8) == 32
+    assert bcn.decode.block_min_len("bc6h", 12) == 48
+    assert bcn.decode.block_min_len("bc6h_float", 12) == 48
+    assert bcn.decode.block_min_len("bc6h_float", 20) == 80  # the slice advances by the pitch after row 4
+    blk = np.zeros(16, np.uint8)
+    out = np.zeros(64, np.uint8)
+    P = lambda a: a.ctypes.data
+    assert L.bc_decode_block_bc1(P(blk), 8, P(out), 63, 16) == -2
+    assert L.bc_decode_block_bc7(P(blk), 15, P(out), 64, 16) == -3
+    assert L.bc_decode_block_bc3(None, 16, P(out), 64, 16) == -6
+    assert L.bc_decode_blocks_device(0, 1, P(blk), 1, P(out), 64, 16, 0, None) == -4
+    assert L.bc_decode_blocks_device(8, 0, P(blk), 1, P(out), 64, 16, 0, None) == -4
+    assert L.bc_decode_blocks_device(7, 0, P(blk), 2, P(out), 64, 8, 40, None) == -2
+    assert L.bc_decode_blocks_device(7, 0, P(blk), 0, P(out), 0, 8, 40, None) == 0
