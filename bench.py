@@ -1,25 +1,36 @@
 """Benchmark: BCn encode throughput on B200 (Mpixel/s).
 
-Workload (one "step"): the 2048x2048 RGBA8 texture-with-alpha workload
-encoded four ways -- BC7 (alpha_basic profile), BC3 and BC4 (R channel) of the
-colour+alpha image, and BC5 of a 2048x2048 normal map -- i.e. 4 x 4.19 Mpx of
-encoded texels per step. Seeded synthetic content (block_compression_b200.
-synthetic); no dataset is involved.
+Workload of the contract line (one "step"): the 2048x2048 RGBA8
+texture-with-alpha image encoded as BC7 (alpha_basic profile), BC3 and BC4 (R
+channel), plus BC5 of a 2048x2048 normal map -- 4 x 4.19 Mpx of encoded
+texels per step. Seeded synthetic content (block_compression_b200/synthetic.py);
+no dataset is involved.
 
 value: encoded Mpixel/s over the whole job (all ranks), device-resident
   inputs, CUDA-event timed per step with an L2 flush (a 256 MiB write)
   before every step.
 e2e:   the same metric through the public host-buffer entry points
-  (bc_compress_rgba8 with pinned host buffers: H2D copy, kernel, D2H copy,
+  (bc_compress_rgba8 with pinned host buffers: H2D copy, kernels, D2H copy,
   synchronize), as a reference user would call compress_rgba8.
 
---impl reference times the reference algorithm on the host CPU (the C++
-restatement of the Rust encoder in oracle/, all host threads) on a bounded
-sample of the same workload.
+The same line carries the other workloads of the metric, each timed with CUDA
+events (L2 flushed before every launch), with its own roofline, CPU baseline
+and full bit-exact check against the CPU oracle:
+  c1  BC1 encode + decode of the 1024x1024 image (HBM roofline; also at
+      8192x8192, where the launch is long enough for the bound to show);
+  c3  BC6H basic encode of the 1024x1024 RGBA16F HDR image (FP32 issue roofline);
+  c4  64 textures with full mip chains, BC1/BC5/BC7 round-robin: the batched
+      CUDA graph against per-task launches, per variant group too.
 
-Multi-GPU: one process per GPU (torchrun); each rank encodes its own copy of
-the workload (independent textures, no data exchange); max-over-ranks device
-time, weak scaling.
+--impl reference times the reference algorithm on the host CPU (the C++
+restatement of the Rust encoder in oracle/, all host threads) on the full
+2048x2048 workload every step; the GPU arm's `cpu_baseline` is the same
+measurement, plus a single-thread figure on a row sample.
+
+Multi-GPU: one process per GPU. Under torchrun the ranks come from the
+environment; `--gpus N` without it starts the N replica processes itself.
+Each rank encodes its own copy of the workload (independent textures, no data
+exchange); max-over-ranks device time, weak scaling.
 """
 import argparse
 import json
@@ -37,14 +48,35 @@ W = H = 2048
 # Algorithmic work per 4x4 block: FP32 operations of the reference encoder
 # (add/sub/mul/div/sqrt/abs/min/max/compare/convert), measured with the
 # op-counting build of the CPU restatement (`python -m oracle.count_ops`,
-# 2048 sampled blocks of this workload's content).
-OPS_PER_BLOCK = {"bc7_alpha_basic": 354530.4, "bc3": 1155.0, "bc4": 101.4, "bc5": 202.3}
+# 2048 sampled blocks of each workload's content).
+OPS_PER_BLOCK = {"bc7_alpha_basic": 354530.4, "bc3": 1155.0, "bc4": 101.4, "bc5": 202.3,
+                 "bc6h_basic": 77119.8, "bc1": 954.3}
 SMS, FP32_LANES_PER_SM = 148, 128
-# DRAM bytes (read + write) of one BC7 encode of this workload, summed over
-# the pipeline's launches, from an ncu capture with warm L2 (--cache-control none).
+# DRAM bytes (read + write) of one BC7 encode of the 2048x2048 workload, summed
+# over the pipeline's launches, from an ncu capture.
 BC7_DRAM_BYTES_PER_LAUNCH = 122.8e6
-METRIC ="BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
+METRIC = "BC7/BC6H/BC1 encode Mpixel/s on 1 B200 at reference PSNR; batched vs plain vs CPU"
 WORKLOAD = "2048x2048 RGBA8 alpha texture: BC7 alpha_basic + BC3 + BC4(R); 2048x2048 normal map: BC5"
+A7 = [2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 12, 8, 8, 0, 2, 4]  # BC7Settings::alpha_basic()
+B6 = [0, 0, 2, 2, 4]                                               # BC6HSettings::basic()
+
+
+def config_dict():
+    """The `config` of both arms' lines (identical keys and values)."""
+    return {"workload": WORKLOAD, "px_per_step": 4 * W * H, "bc7_settings": "alpha_basic",
+            "l2": "GPU arm: flushed (256 MiB write) before each step; CPU arm: not applicable",
+            "seeds": {"image": 2, "normal_map": 2}}
+
+
+def _synthetic():
+    """The seeded generators, loaded by file path: importing the package would
+    load libbcn_b200.so, which the CPU arm must not map."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bcn_synthetic",
+                                                  os.path.join(ROOT, "block_compression_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def _peaks():
@@ -213,51 +245,281 @@ def job_mpx_s(world, px_per_rank_step, steps, ms):
     return world * px_per_rank_step * steps / (ms / 1e3) / 1e6
 
 
+# ---- CPU side: the reference encoder restated in C++ (oracle/) ------------------------
+
+
+def c2_inputs(syn):
+    return {"img": syn.config2_image(seed=2, size=W), "nrm": syn.normal_map(seed=2, size=W)}
+
+
+C2_JOBS = [("bc7_alpha_basic", 6, "img", A7), ("bc3", 2, "img", None), ("bc4", 3, "img", None),
+           ("bc5", 4, "nrm", None)]
+
+
+def cpu_c2_step(oracle, inputs, threads):
+    """One step of the contract workload on the CPU: the four full 2048x2048
+    encodes. Returns (seconds, {job: blocks})."""
+    outs = {}
+    t0 = time.perf_counter()
+    for name, vid, key, s in C2_JOBS:
+        outs[name] = oracle.compress_rgba8(vid, inputs[key], W, H, settings=s, threads=threads)
+    return time.perf_counter() - t0, outs
+
+
+def row_sample(img, every=16):
+    """Every `every`-th row of 4x4 blocks of an image, stacked: a sample
+    spread over the whole image (2048 x 128 for the 2048x2048 inputs)."""
+    rows = [img[y:y + 4] for y in range(0, img.shape[0], 4 * every)]
+    import numpy as np
+    return np.ascontiguousarray(np.concatenate(rows, axis=0))
+
+
+def cpu_c2_single_thread(oracle, inputs):
+    """Mpixel/s of the contract workload on one host thread, on the block-row
+    sample of each input."""
+    sample = {k: row_sample(v) for k, v in inputs.items()}
+    h = sample["img"].shape[0]
+    t0 = time.perf_counter()
+    for name, vid, key, s in C2_JOBS:
+        oracle.compress_rgba8(vid, sample[key], W, h, settings=s, threads=1)
+    return 4 * W * h / (time.perf_counter() - t0) / 1e6
+
+
 def cpu_reference(args, world, rank):
     """Reference arm: the reference's encoder restated in C++ (oracle/), all
-    host threads, on a bounded sample of the workload."""
-    import numpy as np
-
-    import oracle
-    from block_compression_b200 import synthetic
-
+    host threads, on the full contract workload every step."""
     if rank != 0:
         return
-    img = synthetic.config2_image(seed=2, size=W)
-    nrm = synthetic.normal_map(seed=2, size=W)
+    import oracle
+    syn = _synthetic()
+    inputs = c2_inputs(syn)
     threads = os.cpu_count()
-    a7 = [2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 12, 8, 8, 0, 2, 4]  # BC7Settings::alpha_basic()
-    # bounded sample: the full image for BC3/BC4/BC5 and a 256-row band for BC7
-    band = 256
-    crop = np.ascontiguousarray(img[:band])
-
-    def step():
-        t0 = time.perf_counter()
-        oracle.compress_rgba8(6, crop, W, band, settings=a7, threads=threads)
-        t7 = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        oracle.compress_rgba8(2, img, W, H, threads=threads)
-        oracle.compress_rgba8(3, img, W, H, threads=threads)
-        oracle.compress_rgba8(4, nrm, W, H, threads=threads)
-        t345 = time.perf_counter() - t0
-        # full-step time extrapolated from the BC7 band
-        return t7 * (H / band) + t345
-
     for _ in range(max(1, args.warmup)):
-        step()
-    times = [step() for _ in range(args.steps)]
+        cpu_c2_step(oracle, inputs, threads)
+    times = [cpu_c2_step(oracle, inputs, threads)[0] for _ in range(args.steps)]
     t = sum(times) / len(times)
     value = 4 * W * H / t / 1e6
-    sample = "BC7 on a %dx%d band (time scaled x%d), BC3/BC4/BC5 on the full images" % (W, band, H // band)
+    sample = "the full workload every step: BC7 alpha_basic, BC3, BC4 of the 2048x2048 image, BC5 of the normal map"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict(),
         "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---- GPU side ---------------------------------------------------------------------------
+
+
+class DeviceTimer:
+    """CUDA-event times of launches on the current stream, each preceded by
+    an L2 flush (a 256 MiB write, twice the L2)."""
+
+    def __init__(self, torch, dev):
+        self.torch = torch
+        self.flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def time(self, fn, steps, warmup=3):
+        torch = self.torch
+        stream = torch.cuda.current_stream()
+        out = []
+        for i in range(warmup + steps):
+            self.flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            if i >= warmup:
+                out.append(a.elapsed_time(b))
+        return sum(out) / len(out)
+
+
+def hbm_roofline(kernel, nbytes, ms, peaks, src):
+    gbs = nbytes / (ms / 1e3) / 1e9
+    return {"kernel": kernel, "bound": "hbm", "unit": "GB/s", "achieved": gbs, "peak": peaks["hbm_gbs"],
+            "frac": gbs / peaks["hbm_gbs"], "traffic": None, "algorithmic_bytes_per_launch": nbytes,
+            "ms_per_launch": ms, "peak_source": "hbm_gbs (%s)" % src}
+
+
+def issue_roofline(kernel, ops_per_block, nblocks, ms, peaks, src):
+    peak = SMS * FP32_LANES_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved = ops_per_block * nblocks / (ms / 1e3) / 1e12
+    return {"kernel": kernel, "bound": "fp32", "unit": "TFLOP/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "algorithmic_ops_per_block": ops_per_block, "ms_per_launch": ms,
+            "peak_source": "148 SMs x 128 FP32 lanes x %s sm_max_mhz (%s)" % (peaks.get("sm_max_mhz"), src)}
+
+
+def bench_c1(bcn, torch, dev, timer, syn, oracle, steps, peaks, src, verify, cpu):
+    """BC1 encode + decode of the 1024x1024 image (config 1), and the same
+    kernels on the image tiled to 8192x8192 (inputs far beyond L2)."""
+    import numpy as np
+    V = bcn.CompressionVariant
+    img = syn.config1_image(seed=1, size=1024)
+    res = {"workload": "BC1 encode + decode, 1024x1024 RGBA8 (gradients, value noise, 32 triangles), seed 1"}
+    for size, reps in ((1024, 1), (8192, 8)):
+        src_t = torch.from_numpy(np.tile(img, (reps, reps, 1)) if reps > 1 else img).to(dev)
+        blocks = torch.zeros(V.BC1.blocks_byte_size(size, size), dtype=torch.uint8, device=dev)
+        out = torch.zeros(size * size * 4, dtype=torch.uint8, device=dev)
+        enc_ms = timer.time(lambda: bcn.encode.compress_rgba8(V.BC1, src_t, blocks, size, size, size * 4), steps)
+        dec_ms = timer.time(lambda: bcn.decode.decompress_blocks_as_rgba8(V.BC1, size, size, blocks, out), steps)
+        nbytes = size * size * 4 + (size // 4) ** 2 * 8
+        key = "" if size == 1024 else "_8192"
+        res["encode_mpx_s" + key] = size * size / enc_ms / 1e3
+        res["decode_mpx_s" + key] = size * size / dec_ms / 1e3
+        res["roofline_encode" + key] = hbm_roofline("bc15_encode_kernel<BC1>", nbytes, enc_ms, peaks, src)
+        res["roofline_decode" + key] = hbm_roofline("bc15_decode_kernel<BC1>", nbytes, dec_ms, peaks, src)
+        if size == 1024:
+            res["roofline_issue_encode"] = issue_roofline("bc15_encode_kernel<BC1>", OPS_PER_BLOCK["bc1"],
+                                                          (size // 4) ** 2, enc_ms, peaks, src)
+            got_b, got_px = blocks.cpu().numpy(), out.cpu().numpy()
+        del src_t, blocks, out
+    if verify:
+        exp_b = oracle.compress_rgba8(0, img, 1024, 1024)
+        res["verified_full"] = bool(np.array_equal(got_b, exp_b) and
+                                    np.array_equal(got_px, oracle.decompress_rgba8(0, exp_b, 1024, 1024)))
+    if cpu:
+        threads = os.cpu_count()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            b = oracle.compress_rgba8(0, img, 1024, 1024, threads=threads)
+        te = (time.perf_counter() - t0) / 5
+        t0 = time.perf_counter()
+        for _ in range(5):
+            oracle.decompress_rgba8(0, b, 1024, 1024, threads=threads)
+        td = (time.perf_counter() - t0) / 5
+        res["cpu_baseline"] = {"value": 1024 * 1024 / te / 1e6, "unit": "Mpixel/s (encode)",
+                               "decode_mpx_s": 1024 * 1024 / td / 1e6, "cores": threads, "kind": "port",
+                               "sample": "the full 1024x1024 image, 5 passes"}
+    return res
+
+
+def bench_c3(bcn, torch, dev, timer, syn, oracle, steps, peaks, src, verify, cpu):
+    """BC6H basic encode of the 1024x1024 RGBA16F HDR image (config 3)."""
+    import numpy as np
+    s6 = bcn.BC6HSettings.basic()
+    v = bcn.CompressionVariant.BC6H(s6)
+    hdr = syn.config3_hdr(seed=3, size=1024)
+    src_t = torch.from_numpy(hdr.view(np.int16)).to(dev)
+    blocks = torch.zeros(v.blocks_byte_size(1024, 1024), dtype=torch.uint8, device=dev)
+    ms = timer.time(lambda: bcn.encode.compress_rgba16(v, src_t, blocks, 1024, 1024, 1024 * 4), steps)
+    res = {"workload": "BC6H basic encode, 1024x1024 RGBA16F HDR (log-uniform 2^-8..2^8, 2% spikes), seed 3",
+           "encode_mpx_s": 1024 * 1024 / ms / 1e3,
+           "roofline": issue_roofline("bc6h_encode_kernel", OPS_PER_BLOCK["bc6h_basic"], 256 * 256, ms, peaks, src)}
+    got = blocks.cpu().numpy()
+    if verify or cpu:
+        threads = os.cpu_count()
+        t0 = time.perf_counter()
+        exp = oracle.compress_rgba16(hdr.view(np.uint16), 1024, 1024, B6, threads=threads)
+        tc = time.perf_counter() - t0
+        if verify:
+            res["verified_full"] = bool(np.array_equal(got, exp))
+        if cpu:
+            res["cpu_baseline"] = {"value": 1024 * 1024 / tc / 1e6, "unit": "Mpixel/s", "cores": threads,
+                                   "kind": "port", "sample": "the full 1024x1024 image"}
+    return res
+
+
+def bench_c4(bcn, torch, dev, syn, oracle, steps, verify, cpu, textures=64):
+    """Config 4: `textures` RGBA8 textures (sides from {16, 20, ..., 4096}),
+    full GPU-made box-filtered mip chains, BC1 / BC5 / BC7 alpha_basic
+    round-robin; per-task launches against the batched CUDA graph with the
+    autotuned launch shape, for all tasks and per variant group."""
+    import numpy as np
+
+    from block_compression_b200 import mips
+    V = bcn.CompressionVariant
+    variants = [V.BC1, V.BC5, V.BC7(bcn.BC7Settings.alpha_basic())]
+    shapes = syn.config4_textures(seed=4, count=textures)
+    chains = [mips.generate_mip_chain(syn.rgba8_textured_torch(4000 + i, h, w, dev)) for i, (h, w) in
+              enumerate(shapes)]
+    tasks, total = [], 0
+    for i, chain in enumerate(chains):
+        v = variants[i % 3]
+        for li, lv in enumerate(chain):
+            n = v.blocks_byte_size(lv.padded_width, lv.padded_height)
+            tasks.append((lv, v, total, n, li))
+            total += n
+    torch.cuda.synchronize()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def run(sub, out, batched, reps):
+        c = bcn.GpuBlockCompressor()
+        times = []
+        if batched:
+            for lv, v, off, n, _ in sub:
+                c.add_compression_task(v, lv.data, lv.padded_width, lv.padded_height, out, blocks_offset=off)
+            t0 = time.perf_counter()
+            b = c.create_batch(autotune=True)
+            torch.cuda.synchronize()
+            tune_s = time.perf_counter() - t0
+        for i in range(1 + reps):
+            if not batched:
+                for lv, v, off, n, _ in sub:
+                    c.add_compression_task(v, lv.data, lv.padded_width, lv.padded_height, out, blocks_offset=off)
+            a, z = ev(), ev()
+            a.record()
+            b.launch() if batched else c.compress()
+            z.record()
+            torch.cuda.synchronize()
+            if i:
+                times.append(a.elapsed_time(z))
+        extra = {}
+        if batched:
+            extra = {"tune": b.tune.as_dict(), "autotune_s": tune_s}
+            b.close()
+        return sum(times) / len(times), extra
+
+    reps = max(2, min(steps, 5))
+    out_p = torch.zeros(total, dtype=torch.uint8, device=dev)
+    out_b = torch.zeros(total, dtype=torch.uint8, device=dev)
+    px = sum(lv.padded_width * lv.padded_height for lv, _, _, _, _ in tasks)
+    pm, _ = run(tasks, out_p, False, reps)
+    bm, extra = run(tasks, out_b, True, reps)
+    res = {"workload": "%d RGBA8 textures, sides in {16..4096}, full mip chains, BC1/BC5/BC7 alpha_basic "
+                       "round-robin, seed 4" % textures,
+           "tasks": len(tasks), "encoded_mpx": px / 1e6, "plain_ms": pm, "batched_ms": bm,
+           "plain_mpx_s": px / pm / 1e3, "batched_mpx_s": px / bm / 1e3, "batched_over_plain": pm / bm,
+           "outputs_identical": bool(torch.equal(out_p, out_b))}
+    res.update(extra)
+    groups = {}
+    for gname, keep in (("bc7", lambda v: v.id == 6), ("bc1_bc5", lambda v: v.id != 6)):
+        sub = [t for t in tasks if keep(t[1])]
+        gpx = sum(lv.padded_width * lv.padded_height for lv, _, _, _, _ in sub)
+        gp, _ = run(sub, out_p, False, reps)
+        gb, _ = run(sub, out_b, True, reps)
+        groups[gname] = {"tasks": len(sub), "encoded_mpx": gpx / 1e6, "plain_ms": gp, "batched_ms": gb,
+                         "batched_over_plain": gp / gb}
+    res["by_variant"] = groups
+    if verify or cpu:
+        # every level from the 4th down (a spread sample of the chains, about
+        # 1/48 of the pixels): the oracle's blocks against the batched output
+        # and the oracle's time per variant, scaled by each variant's pixels
+        got = out_b.cpu().numpy()
+        threads = os.cpu_count()
+        t_v, px_v, all_px_v, ok = {}, {}, {}, True
+        for lv, v, off, n, li in tasks:
+            all_px_v[v.id] = all_px_v.get(v.id, 0) + lv.padded_width * lv.padded_height
+            if li < 3:
+                continue
+            img = lv.data.cpu().numpy()
+            s = v.settings.as_list() if v.settings is not None else None
+            t0 = time.perf_counter()
+            exp = oracle.compress_rgba8(v.id, img, lv.padded_width, lv.padded_height, settings=s, threads=threads)
+            t_v[v.id] = t_v.get(v.id, 0.0) + time.perf_counter() - t0
+            px_v[v.id] = px_v.get(v.id, 0) + lv.padded_width * lv.padded_height
+            ok = ok and bool(np.array_equal(got[off:off + n], exp))
+        if verify:
+            res["verified_sample"] = ok and res["outputs_identical"]
+        if cpu:
+            est = sum(t_v[k] * all_px_v[k] / px_v[k] for k in t_v)
+            res["cpu_baseline"] = {"value": px / est / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
+                                   "sample": "mip levels 3 and below of every texture (%.1f Mpx), time scaled per "
+                                             "variant by its pixel count" % (sum(px_v.values()) / 1e6)}
+    del chains, out_p, out_b
+    return res
 
 
 def gpu_bench(args, world, rank, local):
@@ -265,7 +527,7 @@ def gpu_bench(args, world, rank, local):
     import torch
 
     import block_compression_b200 as bcn
-    from block_compression_b200 import synthetic
+    syn = _synthetic()
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -280,15 +542,15 @@ def gpu_bench(args, world, rank, local):
     V = bcn.CompressionVariant
     s7 = bcn.BC7Settings.alpha_basic()
     jobs = [("bc7_alpha_basic", V.BC7(s7), "img"), ("bc3", V.BC3, "img"), ("bc4", V.BC4, "img"), ("bc5", V.BC5, "nrm")]
-    img_np = synthetic.config2_image(seed=2, size=W)
-    nrm_np = synthetic.normal_map(seed=2, size=W)
+    inputs = c2_inputs(syn)
+    img_np, nrm_np = inputs["img"], inputs["nrm"]
     srcs = {"img": torch.from_numpy(img_np).to(dev), "nrm": torch.from_numpy(nrm_np).to(dev)}
     outs = {name: torch.zeros(v.blocks_byte_size(W, H), dtype=torch.uint8, device=dev) for name, v, _ in jobs}
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    timer = DeviceTimer(torch, dev)
+    flush = timer.flush
     stream = torch.cuda.current_stream(dev)
-    sptr = stream.cuda_stream
     import ctypes
-    sp = ctypes.c_void_p(sptr)
+    sp = ctypes.c_void_p(stream.cuda_stream)
 
     def run_step(evs=None):
         for i, (name, v, key) in enumerate(jobs):
@@ -354,79 +616,107 @@ def gpu_bench(args, world, rank, local):
     e2e_value = job_mpx_s(world, px_per_step, args.steps, e2e_ms)
     h2d = 3 * img_np.nbytes + nrm_np.nbytes
     d2h = sum(v.blocks_byte_size(W, H) for _, v, _ in jobs)
+    if pg:
+        pg.barrier()
 
-    # correctness guard on the benchmarked output: a sample of blocks vs the oracle
-    import oracle
-    verified = None
     if rank == 0:
-        rng = np.random.default_rng(0)
-        bw = W // 4
-        idx = rng.choice((W // 4) * (H // 4), 64, replace=False)
-        tiles = np.stack([img_np[(i // bw) * 4:(i // bw) * 4 + 4, (i % bw) * 4:(i % bw) * 4 + 4] for i in idx])
-        tile_img = np.ascontiguousarray(tiles.transpose(1, 0, 2, 3).reshape(4, 64 * 4, 4))
-        exp = oracle.compress_rgba8(6, tile_img, 256, 4, settings=s7.as_list()).reshape(64, 16)
-        got = outs["bc7_alpha_basic"].cpu().numpy().reshape(-1, 16)[idx]
-        verified = bool(np.array_equal(exp, got))
-
-    # CPU baseline (rank 0, N=1): bounded sample on all host threads
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        threads = os.cpu_count()
-        band = 128
-        crop = np.ascontiguousarray(img_np[:band])
-        t0 = time.perf_counter()
-        oracle.compress_rgba8(6, crop, W, band, settings=s7.as_list(), threads=threads)
-        t7 = (time.perf_counter() - t0) * (H / band)
-        t0 = time.perf_counter()
-        oracle.compress_rgba8(2, img_np, W, H, threads=threads)
-        oracle.compress_rgba8(3, img_np, W, H, threads=threads)
-        oracle.compress_rgba8(4, nrm_np, W, H, threads=threads)
-        t345 = time.perf_counter() - t0
-        cpu = {"value": px_per_step / (t7 + t345) / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
-               "sample": "BC7 on a %dx%d band scaled to the full image; BC3/BC4/BC5 full" % (W, band)}
-
-    peaks, src = _peaks()
-    bc7_ms = sum(per_job["bc7_alpha_basic"]) / len(per_job["bc7_alpha_basic"])
-    bc3_ms = sum(per_job["bc3"]) / len(per_job["bc3"])
-    if rank == 0:
+        import oracle
+        peaks, src = _peaks()
+        verify = not args.no_verify
+        cpu_leg = world == 1 and not args.no_cpu
+        # the oracle's outputs of the whole workload: the full bit-exact check
+        # of every encoded block, and (one rank, one GPU) the CPU baseline
+        cpu, verified = None, None
+        if verify or cpu_leg:
+            threads = os.cpu_count()
+            tc, exp = cpu_c2_step(oracle, inputs, threads)
+            verified = {name: bool(np.array_equal(outs[name].cpu().numpy(), exp[name])) for name, _, _ in jobs}
+            verified["host_entry_points"] = all(bool(np.array_equal(host_out[name], exp[name])) for name, _, _ in jobs)
+            if cpu_leg:
+                cpu = {"value": px_per_step / tc / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
+                       "sample": "the full workload (same measurement as the reference arm): BC7 alpha_basic, BC3, "
+                                 "BC4 of the 2048x2048 image, BC5 of the normal map",
+                       "single_thread": {"value": cpu_c2_single_thread(oracle, inputs), "unit": "Mpixel/s",
+                                         "cores": 1, "sample": "every 16th row of blocks of each input (2048x128)"}}
+        bc7_ms = sum(per_job["bc7_alpha_basic"]) / len(per_job["bc7_alpha_basic"])
         per_variant = {name: W * H / (sum(ms) / len(ms) / 1e3) / 1e6 for name, ms in per_job.items()}
-        # BC7 is compute bound: algorithmic FP32 ops per launch / duration,
-        # against the FP32 issue rate (148 SMs x 128 lanes x max SM clock; the
-        # encoder's order-preserving arithmetic admits no FMA).
         nblk = (W // 4) * (H // 4)
-        fp32_peak = SMS * FP32_LANES_PER_SM * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-        achieved = OPS_PER_BLOCK["bc7_alpha_basic"] * nblk / (bc7_ms / 1e3) / 1e12
-        roof = {
-            "kernel": "BC7 encode pipeline (bc7_prep/search/refine/mode45/mode6/select)", "bound": "fp32",
-            "unit": "TFLOP/s", "achieved": achieved, "peak": fp32_peak, "frac": achieved / fp32_peak,
-            "peak_source": "148 SMs x 128 FP32 lanes x %s sm_max_mhz (%s)" % (peaks.get("sm_max_mhz"), src),
-            "traffic": BC7_DRAM_BYTES_PER_LAUNCH, "algorithmic_ops_per_block": OPS_PER_BLOCK["bc7_alpha_basic"],
-            "ms_per_launch": bc7_ms,
-        }
-        bc3_bytes = W * H * 4 + (W // 4) * (H // 4) * 16
-        hbm = {"kernel": "bc15_encode_kernel<BC3>", "bound": "hbm", "unit": "GB/s",
-               "achieved": bc3_bytes / (bc3_ms / 1e3) / 1e9, "peak": peaks["hbm_gbs"],
-               "frac": bc3_bytes / (bc3_ms / 1e3) / 1e9 / peaks["hbm_gbs"], "peak_source": src}
+        roof = issue_roofline("BC7 encode pipeline (bc7_prep/search/refine/mode45/mode6/select)",
+                              OPS_PER_BLOCK["bc7_alpha_basic"], nblk, bc7_ms, peaks, src)
+        roof["traffic"] = BC7_DRAM_BYTES_PER_LAUNCH
+        hbm = {}
+        for name in ("bc3", "bc4", "bc5"):
+            ms = sum(per_job[name]) / len(per_job[name])
+            nbytes = W * H * 4 + nblk * (8 if name == "bc4" else 16)
+            hbm[name] = hbm_roofline("bc15_encode_kernel<%s>" % name.upper(), nbytes, ms, peaks, src)
+        extra = {}
+        if not args.no_extra:
+            extra["c1"] = bench_c1(bcn, torch, dev, timer, syn, oracle, max(3, args.steps), peaks, src, verify,
+                                   cpu_leg)
+            extra["c3"] = bench_c3(bcn, torch, dev, timer, syn, oracle, max(3, args.steps), peaks, src, verify,
+                                   cpu_leg)
+            extra["c4"] = bench_c4(bcn, torch, dev, syn, oracle, args.steps, verify, cpu_leg)
         line = {
             "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "px_per_step": px_per_step, "l2": "flushed (256 MiB write) before each step",
-                       "bc7_settings": "alpha_basic"},
+            "config": config_dict(),
             "e2e": {"value": e2e_value, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             # our kernels in the timed region: the BC7 pipeline plus one
             # kernel each for BC3, BC4 and BC5, per step
             "gpu_launches": (bc7_kernel_count(s7) + len(jobs) - 1) * args.steps,
             "per_variant_mpx_s": per_variant,
-            "roofline": roof, "roofline_hbm_path": hbm,
+            "roofline": roof, "roofline_hbm_paths": hbm,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "verified_bc7_sample": verified,
+            "verified_full": verified,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def _free_port():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_replicas(n, argv):
+    """Starts `n` processes of this script, one per GPU (rank i on GPU i),
+    with the rendezvous environment torchrun would set; returns the worst
+    exit status. Only rank 0 prints."""
+    port = _free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + argv, env=env))
+    rcs = [p.wait() for p in procs]
+    return max(rcs, key=abs)
+
+
+def ranks_selftest(args, world, rank):
+    """The replica plumbing alone, on the CPU: rendezvous (gloo), barrier,
+    max-over-ranks of a per-rank time, the whole-job throughput. Rank 0
+    prints one line. Used by the multi-rank CPU test."""
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    try:
+        dist.barrier()
+        my_ms = 10.0 + 5.0 * rank
+        ms = max_over_ranks(my_ms, dist, "cpu")
+        if rank == 0:
+            print(json.dumps({"world": world, "max_ms": ms, "mpx_s": job_mpx_s(world, 4 * W * H, 10, ms)}),
+                  flush=True)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
 
 
 def profile_case(args):
@@ -690,22 +980,30 @@ def decode_bench(args):
     print(json.dumps(out), flush=True)
 
 
-def main():
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline legs")
+    ap.add_argument("--no-verify", action="store_true", help="skip the bit-exact checks against the oracle")
+    ap.add_argument("--no-extra", action="store_true", help="only the contract workload (no c1/c3/c4 objects)")
     ap.add_argument("--case", default=None, help="profiling case VARIANT:SIZE, e.g. bc7:512 (not a bench line)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "mips", "refine", "decode"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "mips", "refine", "decode", "ranks"],
                     help="c2: the benchmark line; mips: batched mixed mip-chain workload; refine: gradient "
-                         "endpoint refinement; decode: decode bandwidth (extra lines)")
+                         "endpoint refinement; decode: decode bandwidth (extra lines); ranks: the replica "
+                         "plumbing on CPU (gloo)")
     ap.add_argument("--textures", type=int, default=64)
     ap.add_argument("--decode-size", type=int, default=8192)
-    args = ap.parse_args()
+    args = ap.parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_replicas(args.gpus, argv)
     world, rank, local = _dist()
-    if args.case:
+    if args.workload == "ranks":
+        ranks_selftest(args, world, rank)
+    elif args.case:
         profile_case(args)
     elif args.workload == "mips":
         batched_mips_bench(args)
@@ -717,7 +1015,8 @@ def main():
         cpu_reference(args, world, rank)
     else:
         gpu_bench(args, world, rank, local)
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

@@ -48,3 +48,21 @@ def test_single_process_needs_no_group():
     import bench
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
     assert bench.job_mpx_s(1, 1_000_000, 2, 1000.0) == pytest.approx(2.0)
+
+
+def test_bench_starts_its_own_replicas():
+    """`bench.py --gpus 2` without a launcher's environment starts two rank
+    processes itself (as it does for N GPUs); the replica plumbing alone
+    (rendezvous, barrier, max-over-ranks) runs here on gloo."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--workload", "ranks", "--gpus", "2"],
+                       capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1  # rank 0 alone prints
+    assert lines[0]["world"] == 2 and lines[0]["max_ms"] == 15.0
+    assert lines[0]["mpx_s"] == pytest.approx(2 * 4 * 2048 * 2048 * 10 / 0.015 / 1e6)
