@@ -58,6 +58,8 @@ def lib():
         L.oracle_block_pca_bound_split.restype = ctypes.c_float
         L.oracle_block_segment_core.argtypes = [P, P, U32, U32]
         L.oracle_block_segment_core.restype = None
+        L.oracle_ep_quant_dequant.argtypes = [P, P, U32, U32]
+        L.oracle_ep_quant_dequant.restype = None
         for name in ("oracle_get_pattern", "oracle_get_skip_packed"):
             getattr(L, name).argtypes = [ctypes.c_int32]
             getattr(L, name).restype = U32

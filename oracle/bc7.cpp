@@ -539,6 +539,11 @@ void bc7_encode_block(const real block[64], const BC7Settings* settings, uint32_
     for (int i = 0; i < 4; i++) out[i] = s.data[i];
 }
 
+// bc7.rs:234-237, exported for the differential tests.
+void bc7_ep_quant_dequant(int32_t* qep, real* ep, uint32_t mode, uint32_t channels) {
+    ep_quant_dequant(qep, ep, mode, channels);
+}
+
 }  // namespace oracle
 
 #ifndef ORACLE_COUNT_OPS

@@ -317,6 +317,9 @@ extern "C" float oracle_block_pca_bound_split(const float* block, uint32_t mask,
 extern "C" void oracle_block_segment_core(float* ep, const float* block, uint32_t mask, uint32_t channels) {
     block_segment_core(ep, block, mask, channels);
 }
+extern "C" void oracle_ep_quant_dequant(int32_t qep[24], float ep[24], uint32_t mode, uint32_t channels) {
+    bc7_ep_quant_dequant(qep, ep, mode, channels);
+}
 extern "C" uint32_t oracle_get_pattern(int32_t part_id) { return get_pattern(part_id); }
 extern "C" uint32_t oracle_get_pattern_mask(int32_t part_id, uint32_t j) { return get_pattern_mask(part_id, j); }
 extern "C" uint32_t oracle_get_skip_packed(int32_t part_id) { return kSkipTable[part_id]; }

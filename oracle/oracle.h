@@ -59,6 +59,8 @@ void oracle_opt_endpoints(float* ep, const float* block, uint32_t bits, const ui
                           uint32_t mask, uint32_t channels);
 float oracle_block_pca_bound_split(const float* block, uint32_t mask, uint32_t channels);
 void oracle_block_segment_core(float* ep, const float* block, uint32_t mask, uint32_t channels);
+/* ep_quant_dequant of src/encode/bc7.rs:234 (24 endpoint values, mode 0-7). */
+void oracle_ep_quant_dequant(int32_t qep[24], float ep[24], uint32_t mode, uint32_t channels);
 uint32_t oracle_get_pattern(int32_t part_id);
 uint32_t oracle_get_pattern_mask(int32_t part_id, uint32_t j);
 uint32_t oracle_get_skip_packed(int32_t part_id);

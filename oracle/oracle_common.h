@@ -124,6 +124,7 @@ real block_pca_bound_split(const real block[64], uint32_t mask, const real full_
 real block_quant(uint32_t qblock[2], const real block[64], uint32_t bits, const real* ep,
                   uint32_t pattern, uint32_t channels);             // common.rs:422
 void block_segment_core(real* ep, const real block[64], uint32_t mask, uint32_t channels);
+void bc7_ep_quant_dequant(int32_t* qep, real* ep, uint32_t mode, uint32_t channels);  // bc7.rs:234
 void bc7_code_qblock(uint32_t data[5], uint32_t* qpos, const uint32_t qblock[2], uint32_t bits,
                      uint32_t flips);                               // common.rs:520
 void bc7_code_adjust_skip_mode01237(uint32_t data[5], uint32_t mode, int32_t part_id);
