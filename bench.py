@@ -409,6 +409,8 @@ def bench_c3(bcn, torch, dev, timer, syn, oracle, steps, peaks, src, verify, cpu
            "encode_mpx_s": 1024 * 1024 / ms / 1e3,
            "roofline": issue_roofline("bc6h_encode_kernel", OPS_PER_BLOCK["bc6h_basic"], 256 * 256, ms, peaks, src)}
     got = blocks.cpu().numpy()
+    from block_compression_b200 import metrics
+    res["log_luminance_rmse"] = metrics.log_luminance_rmse(src_t, blocks, 1024, 1024)
     if verify or cpu:
         threads = os.cpu_count()
         t0 = time.perf_counter()
@@ -416,6 +418,19 @@ def bench_c3(bcn, torch, dev, timer, syn, oracle, steps, peaks, src, verify, cpu
         tc = time.perf_counter() - t0
         if verify:
             res["verified_full"] = bool(np.array_equal(got, exp))
+            # FP64 recomputation of every block's squared error, ours against
+            # the reference's blocks, and the reference's log-luminance RMSE
+            exp_t = torch.from_numpy(exp).to(dev)
+            sse_g = torch.zeros(256 * 256, dtype=torch.float64, device=dev)
+            sse_r = torch.zeros(256 * 256, dtype=torch.float64, device=dev)
+            metrics.bc6h_error(src_t, blocks, 1024, 1024, block_sse=sse_g)
+            metrics.bc6h_error(src_t, exp_t, 1024, 1024, block_sse=sse_r)
+            excess = ((sse_g - sse_r) / sse_r.clamp_min(1e-300)).max().item()
+            res["quality"] = {
+                "log_luminance_rmse_reference": metrics.log_luminance_rmse(src_t, exp_t, 1024, 1024),
+                "blocks_bit_identical": float((got.reshape(-1, 16) == exp.reshape(-1, 16)).all(1).mean()),
+                "max_block_sse_excess_rel": max(0.0, excess),
+                "metric": "RGB squared error and log2 Rec.709 luminance error in f64 (bc_bc6h_error_device)"}
         if cpu:
             res["cpu_baseline"] = {"value": 1024 * 1024 / tc / 1e6, "unit": "Mpixel/s", "cores": threads,
                                    "kind": "port", "sample": "the full 1024x1024 image"}

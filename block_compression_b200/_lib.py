@@ -89,6 +89,7 @@ def _load():
         "bc_bc7_refine_images_device": ([P, U32, U32, U32, ctypes.c_float, P, P], I),
         "bc_bc1_refine_images_device": ([P, U32, U32, ctypes.c_float, P, P], I),
         "bc_image_sse_rgba8_device": ([P, S, P, S, U32, U32, U32, P, P], I),
+        "bc_bc6h_error_device": ([P, S, S, P, S, U32, U32, P, P, P], I),
         "bc_dds_header": ([I, U32, U32, U32, I, P, S], I),
         "bc_dds_dxgi_format": ([I, I], U32),
         "bc_last_cuda_error": ([], I),

@@ -5,7 +5,7 @@
 //   BC1-BC5 tasks  one persistent work-queue launch over all their tiles
 //   BC7 tasks      one pass of the BC7 pipeline over all tiles of all tasks
 //                  that share settings (each phase is a single launch)
-//   BC6H tasks     one launch per task
+//   BC6H tasks     one pass of the BC6H kernel pipeline per task
 //
 // The launch shape (threads per CTA, resident CTAs per SM, tiles per
 // work-queue claim, candidates per BC7 search CTA) comes from a bc_tune
@@ -97,8 +97,8 @@ int enqueue(bc_batch* b, const bc_tune& t, cudaStream_t s, int which) {
                                         (int)t.bc7_search_warps, s));
         } else {
             const BcTaskView& v = g.task;
-            launch_bc6h_encode(v.src, v.pitch, BC6H_SRC_RGBA16F, (v.w + 3) / 4, (v.h + 3) / 4, v.dst, g.s6, s);
-            BATCH_CUDA(cudaGetLastError());
+            BATCH_CUDA(launch_bc6h_encode(v.src, v.pitch, BC6H_SRC_RGBA16F, (v.w + 3) / 4, (v.h + 3) / 4, v.dst,
+                                          g.s6, b->d_scratch, s));
         }
     }
     return BC_OK;
@@ -282,6 +282,8 @@ extern "C" int bc_batch_create(bc_compressor* c, const bc_tune* tune, int autotu
         g.kind = 2;
         g.s6 = *(const BC6HSettingsDev*)v.settings;
         g.task = v;
+        size_t need = bc6h_scratch_bytes(((v.w + 3) / 4) * ((v.h + 3) / 4), g.s6);
+        if (need > max_scratch) max_scratch = need;
         b->groups.push_back(g);
     }
     compressor_clear(c);

@@ -1,26 +1,31 @@
 // BC6H (unsigned float) encoder for sm_100a.
 //
-// Same tiling as the BC7 kernel: a CTA owns 32 consecutive blocks, lane l of
-// every warp works on block l. The reference's per-block search
-// (src/encode/bc6h.rs:288-860) is a sequence of "encodes", each run with a
-// per-block quantisation state (mode, endpoint bits, quantisation bounds)
-// chosen by bc6h_test_mode's span checks:
+// Work decomposition as in the BC7 encoder: tiles of 32 consecutive blocks,
+// lane l of a warp always works on block l of its tile. The reference's
+// per-block search (src/encode/bc6h.rs:288-860) is a sequence of "encodes",
+// each run with a per-block quantisation state (mode, endpoint bits,
+// quantisation bounds) chosen by bc6h_test_mode's span checks:
 //   fast/basic settings: one 2-region encode in the mode the tests settle on,
 //                        one 2-region encode in mode 1 (not in fast mode), and
 //                        one 1-region encode;
 //   slow settings:       2-region encodes in modes 0,1,2,5,6,9 and 1-region
 //                        encodes in modes 10..13.
-// Phases:
-//   1. load + setup    f16 bit patterns -> f32, scaled by 64/31, block bounds,
-//                      per-block states of every encode
-//   2. bounds          32 PCA split bounds per block (mode independent, so one
-//                      pass serves every 2-region encode)
-//   3. top-k           ascending partial sort of the 32 bounds
-//   4. search          (encode, partition) candidates spread over warps; each
-//                      warp keeps a first minimum per encode
-//   5. chains          refinement + coding of each 2-region encode's winner,
-//                      and each 1-region encode
-//   6. select          the reference's sequential strict comparisons
+// It runs as a pipeline of launches, each one code path (a single fused
+// kernel ran at 42% issue: 164 registers, local-memory arrays, warps idle at
+// the barriers between unequal phases):
+//   prep     setup (bc6h.rs:793-819) and the encode states of every block,
+//            the 32 PCA split bounds and the ascending top-k partition list
+//   search   grid (tile, candidate group): a warp evaluates one (2-region
+//            encode, partition) candidate for 32 blocks; the first minimum
+//            per block and encode is kept with a 64-bit atomicMin on
+//            (error bits << 32 | candidate)
+//   refine2  one warp per (tile, 2-region encode): refinement of the winner
+//            and coding
+//   enc1     one warp per (tile, 1-region encode)
+//   select   the reference's sequential strict comparisons -> 128-bit store
+// Per-block state between launches lives in scratch device memory
+// (bc6h_scratch_bytes), indexed [row * npad + block] so a warp's lanes touch
+// consecutive entries.
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 
@@ -45,12 +50,20 @@ namespace bc6h {
 using namespace bptc;
 
 // Minimum resident CTAs per SM requested from the register allocator.
-#ifndef BCN_BC6H_MINB
-#define BCN_BC6H_MINB 3
+#ifndef BCN_BC6H_PREP_MINB
+#define BCN_BC6H_PREP_MINB 4
+#endif
+#ifndef BCN_BC6H_SEARCH_MINB
+#define BCN_BC6H_SEARCH_MINB 5
+#endif
+#ifndef BCN_BC6H_REFINE_MINB
+#define BCN_BC6H_REFINE_MINB 4
+#endif
+#ifndef BCN_BC6H_ENC1_MINB
+#define BCN_BC6H_ENC1_MINB 4
 #endif
 
-constexpr int MAXJ = 10;  // encodes per block (slow settings)
-constexpr int NW = 4;
+constexpr int NW = 4;     // warps per CTA
 
 struct Job {  // per-block quantisation state of one encode
     int mode;
@@ -58,19 +71,24 @@ struct Job {  // per-block quantisation state of one encode
     int qb[6];  // qbounds[0..3) and qbounds[4..7)
 };
 
-struct Smem {
-    float px[48][NB];
-    int keys[32][NB];
-    uint8_t list[32][NB];
-    int jmode[MAXJ][NB];
-    int jepb[MAXJ][NB];
-    int jqb[MAXJ][6][NB];
-    float werr[6][NW][NB];
-    int wcand[6][NW][NB];
-    int winner[6][NB];
-    float slot_err[MAXJ][NB];
-    uint4 slot_data[MAXJ][NB];
-};
+// A job in 16 bytes: mode | epb << 8, then the six bounds as 16-bit pairs
+// (a bound is at most 2^16 - 1).
+BCN_DEV uint4 pack_job(const Job& j) {
+    return make_uint4((uint32_t)j.mode | ((uint32_t)j.epb << 8), (uint32_t)j.qb[0] | ((uint32_t)j.qb[1] << 16),
+                      (uint32_t)j.qb[2] | ((uint32_t)j.qb[3] << 16), (uint32_t)j.qb[4] | ((uint32_t)j.qb[5] << 16));
+}
+BCN_DEV Job unpack_job(uint4 v) {
+    Job j;
+    j.mode = (int)(v.x & 0xFFu);
+    j.epb = (int)(v.x >> 8);
+    j.qb[0] = (int)(v.y & 0xFFFFu);
+    j.qb[1] = (int)(v.y >> 16);
+    j.qb[2] = (int)(v.z & 0xFFFFu);
+    j.qb[3] = (int)(v.z >> 16);
+    j.qb[4] = (int)(v.w & 0xFFFFu);
+    j.qb[5] = (int)(v.w >> 16);
+    return j;
+}
 
 // bc6h.rs:137-164
 BCN_DEV float get_span(int mode) {
@@ -375,11 +393,14 @@ BCN_DEV float eval_2p(const Blk& blk, int part_id, int epb, const int qb[6], int
     return block_quant<3, 3, 2>(blk, ep, pattern, q0, q1);
 }
 
-// bc6h.rs:355-387 (refine) + bc6h_code_2p (bc6h.rs:241-266)
-BCN_DEV float refine_code_2p(const Blk& blk, int part_id, const Job& st, float best_err, uint32_t iters, uint4& out) {
-    int best_qep[24];
-    uint32_t bq0, bq1;
-    eval_2p(blk, part_id, st.epb, st.qb, best_qep, bq0, bq1);
+// The refinement of a two-region encode's winner (bc6h.rs:355-387): the
+// best endpoints (qep[0..16), channel 3 unused) and indices.
+BCN_DEV float refine_2p(const Blk& blk, int part_id, const Job& st, float best_err, uint32_t iters,
+                        int best_qep[16], uint32_t& bq0, uint32_t& bq1) {
+    int qe[24];
+    eval_2p(blk, part_id, st.epb, st.qb, qe, bq0, bq1);
+#pragma unroll
+    for (int i = 0; i < 16; i++) best_qep[i] = qe[i];
     uint32_t pattern = kPartitionMap[part_id];
     for (uint32_t it = 0; it < iters; it++) {
         float ep[24];
@@ -399,9 +420,14 @@ BCN_DEV float refine_code_2p(const Blk& blk, int part_id, const Job& st, float b
             best_err = err;
         }
     }
-    uint32_t flips = apply_swap_mode01237(best_qep, bq0, bq1, 1, part_id);
+    return best_err;
+}
+
+// bc6h_code_2p (bc6h.rs:241-266).
+BCN_DEV uint4 code_2p(int qep[24], uint32_t q0, uint32_t q1, int part_id, int mode) {
+    uint32_t flips = apply_swap_mode01237(qep, q0, q1, 1, part_id);
     uint32_t packed[4];
-    bc6h_pack(packed, best_qep, st.mode);
+    bc6h_pack(packed, qep, mode);
     BitWriter bw;
     bw.clear();
     bw.put(5, packed[0]);
@@ -409,14 +435,13 @@ BCN_DEV float refine_code_2p(const Blk& blk, int part_id, const Job& st, float b
     bw.put(30, packed[2]);
     bw.put(12, packed[3]);
     bw.put(5, (uint32_t)part_id);
-    code_qblock(bw, bq0, bq1, 3, flips);
+    code_qblock(bw, q0, q1, 3, flips);
     adjust_skip_mode01237(bw.d, 1, part_id);
-    out = make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
-    return best_err;
+    return make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
 }
 
-// bc6h_enc_1p (bc6h.rs:390-412) + bc6h_code_1p (bc6h.rs:268-286)
-BCN_DEV float encode_1p(const Blk& blk, const Job& st, uint32_t iters, uint4& out) {
+// bc6h_enc_1p (bc6h.rs:390-412): the endpoints (qep[0..8)) and indices.
+BCN_DEV float encode_1p(const Blk& blk, const Job& st, uint32_t iters, int out_qep[8], uint32_t& q0, uint32_t& q1) {
     float ep[24];
 #pragma unroll
     for (int i = 0; i < 24; i++) ep[i] = 0.0f;
@@ -425,78 +450,130 @@ BCN_DEV float encode_1p(const Blk& blk, const Job& st, uint32_t iters, uint4& ou
 #pragma unroll
     for (int i = 0; i < 24; i++) qep[i] = 0;
     quant_dequant<1>(qep, ep, st.epb, st.qb);
-    uint32_t q0, q1;
     float err = block_quant<3, 4, 1>(blk, ep, 0, q0, q1);
     for (uint32_t it = 0; it < iters; it++) {
         opt_endpoints<3, 4>(ep, blk, q0, q1, 0xFFFFu);
         quant_dequant<1>(qep, ep, st.epb, st.qb);
         err = block_quant<3, 4, 1>(blk, ep, 0, q0, q1);
     }
+#pragma unroll
+    for (int i = 0; i < 8; i++) out_qep[i] = qep[i];
+    return err;
+}
+
+// bc6h_code_1p (bc6h.rs:268-286).
+BCN_DEV uint4 code_1p(int qep[24], uint32_t q0, uint32_t q1, int mode) {
     apply_swap_mode456(qep, 4, q0, q1, 4);
     uint32_t packed[4];
-    bc6h_pack(packed, qep, st.mode);
+    bc6h_pack(packed, qep, mode);
     BitWriter bw;
     bw.clear();
     bw.put(5, packed[0]);
     bw.put(30, packed[1]);
     bw.put(30, packed[2]);
     code_qblock(bw, q0, q1, 4, 0);
-    out = make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
-    return err;
+    return make_uint4(bw.d[0], bw.d[1], bw.d[2], bw.d[3]);
 }
 
 // Encode list of a settings value: kind (2 = two-region, 1 = one-region) per
-// encode, in the reference's order. Uniform over the launch.
+// encode, in the reference's order (the two-region encodes come first).
+// Uniform over the launch.
 struct Plan {
     int n;
-    int kind[MAXJ];
-    int n2;  // number of two-region encodes (they come first)
+    int n2;  // number of two-region encodes
     int k;   // partitions tried per two-region encode
 };
 
-BCN_DEV Plan make_plan(const BC6HSettingsDev& s) {
+static __host__ __device__ Plan make_plan(const BC6HSettingsDev& s) {
     Plan p;
-    p.n = 0;
     if (s.slow_mode != 0) {
-        for (int i = 0; i < 6; i++) p.kind[p.n++] = 2;
-        for (int i = 0; i < 4; i++) p.kind[p.n++] = 1;
+        p.n2 = 6;
+        p.n = 10;
     } else {
-        if (s.fast_skip_threshold > 0) {
-            p.kind[p.n++] = 2;
-            if (s.fast_mode == 0) p.kind[p.n++] = 2;
-        }
-        p.kind[p.n++] = 1;
+        p.n2 = s.fast_skip_threshold > 0 ? (s.fast_mode == 0 ? 2 : 1) : 0;
+        p.n = p.n2 + 1;
     }
-    p.n2 = 0;
-    for (int i = 0; i < p.n; i++) p.n2 += p.kind[i] == 2;
     p.k = (int)s.fast_skip_threshold;
+    if (p.k == 0) {  // no partition is tried: the 2-region encodes do nothing (bc6h.rs:327-329)
+        p.n2 = 0;
+        p.n = s.slow_mode != 0 ? 4 : 1;
+    }
     return p;
 }
 
-__global__ void __launch_bounds__(NW * 32, BCN_BC6H_MINB) bc6h_encode_kernel(const uint8_t* __restrict__ src, size_t stride,
-                                                               int source_format, uint32_t bw, uint32_t nblocks,
-                                                               uint8_t* __restrict__ dst, BC6HSettingsDev S) {
-    __shared__ Smem sm;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile0 = blockIdx.x * NB;
-    const Plan P = make_plan(S);
+// Arguments shared by every kernel of one encode.
+struct Work {
+    const uint8_t* src;
+    size_t stride;
+    int source_format;
+    bool aligned;  // 16-byte loads of RGBA16F rows
+    uint32_t bw, nblocks, npad;
+    uint8_t* dst;
+    uint4* jobs;               // [j * npad + block]
+    uint8_t* lists;            // [c * npad + block]: top-k partitions, ascending bound
+    unsigned long long* keys;  // [j * npad + block], 2-region encodes: (error bits << 32) | candidate
+    float* slot_err;           // [j * npad + block]
+    uint4* slot_pay;           // [(j * 3 + r) * npad + block]: the encode's result, coded by select only if it wins
+    BC6HSettingsDev S;
+};
 
-    // 1. load: f16 bit patterns as f32 (bc6h.rs:73-97 / 45-71)
-    for (int t = threadIdx.x; t < NB * 4; t += blockDim.x) {
-        int b = t & 31, y = t >> 5;
-        uint32_t gi = tile0 + b;
+// An encode's result in three 16-byte rows: the 16 endpoint values as 16-bit
+// pairs (BC6H endpoints are below 2^16), then the indices and the partition.
+BCN_DEV void store_pay(const Work& w, int j, uint32_t gi, const int qep[16], uint32_t q0, uint32_t q1, int part) {
+    uint32_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = (uint32_t)qep[2 * i] | ((uint32_t)qep[2 * i + 1] << 16);
+    w.slot_pay[((size_t)j * 3 + 0) * w.npad + gi] = make_uint4(v[0], v[1], v[2], v[3]);
+    w.slot_pay[((size_t)j * 3 + 1) * w.npad + gi] = make_uint4(v[4], v[5], v[6], v[7]);
+    w.slot_pay[((size_t)j * 3 + 2) * w.npad + gi] = make_uint4(q0, q1, (uint32_t)part, 0u);
+}
+BCN_DEV void load_pay(const Work& w, int j, uint32_t gi, int qep[24], uint32_t& q0, uint32_t& q1, int& part) {
+    const uint4 a = w.slot_pay[((size_t)j * 3 + 0) * w.npad + gi], b = w.slot_pay[((size_t)j * 3 + 1) * w.npad + gi],
+                c = w.slot_pay[((size_t)j * 3 + 2) * w.npad + gi];
+    const uint32_t v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        qep[2 * i] = (int)(v[i] & 0xFFFFu);
+        qep[2 * i + 1] = (int)(v[i] >> 16);
+    }
+#pragma unroll
+    for (int i = 16; i < 24; i++) qep[i] = 0;
+    q0 = c.x;
+    q1 = c.y;
+    part = (int)c.z;
+}
+
+// Stages the 32 blocks of `tile` as planar f32 (the f16 bit pattern of
+// every channel value, scaled by 64/31 as bc6h_setup does, bc6h.rs:801-804)
+// with threads tid = 0..nt-1 of the caller; px rows are c * 16 + k.
+BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, int nt) {
+    for (int t = tid; t < NB * 4; t += nt) {
+        const int b = t & 31, y = t >> 5;
+        const uint32_t gi = tile * NB + b;
         float v[12];
 #pragma unroll
         for (int i = 0; i < 12; i++) v[i] = 0.0f;
-        if (gi < nblocks) {
-            uint32_t by = gi / bw, bx = gi - by * bw;
-            const uint8_t* row = src + (size_t)(by * 4 + y) * stride;
-            if (source_format == BC6H_SRC_RGBA16F) {
-                const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row) + (size_t)bx * 16;
+        if (gi < w.nblocks) {
+            const uint32_t by = gi / w.bw, bx = gi - by * w.bw;
+            const uint8_t* row = w.src + (size_t)(by * 4 + y) * w.stride;
+            if (w.source_format == BC6H_SRC_RGBA16F) {
+                if (w.aligned) {  // the row's 4 pixels: 32 bytes
+                    const uint4* r = reinterpret_cast<const uint4*>(row + (size_t)bx * 32);
+                    const uint4 a = __ldg(r), c = __ldg(r + 1);
+                    const uint32_t wd[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
 #pragma unroll
-                for (int x = 0; x < 4; x++)
+                    for (int x = 0; x < 4; x++) {
+                        v[x * 3 + 0] = (float)(wd[2 * x] & 0xFFFFu);
+                        v[x * 3 + 1] = (float)(wd[2 * x] >> 16);
+                        v[x * 3 + 2] = (float)(wd[2 * x + 1] & 0xFFFFu);
+                    }
+                } else {
+                    const uint16_t* r16 = reinterpret_cast<const uint16_t*>(row) + (size_t)bx * 16;
 #pragma unroll
-                    for (int c = 0; c < 3; c++) v[x * 3 + c] = (float)r16[x * 4 + c];
+                    for (int x = 0; x < 4; x++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) v[x * 3 + c] = (float)r16[x * 4 + c];
+                }
             } else {
                 const uint8_t* r8 = row + (size_t)bx * 16;
 #pragma unroll
@@ -508,212 +585,338 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_MINB) bc6h_encode_kernel(con
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) sm.px[c * 16 + y * 4 + x][b] = div_const<31>(v[x * 3 + c]) * 64.0f;
+            for (int c = 0; c < 3; c++) px[c * 16 + y * 4 + x][b] = div_const<31>(v[x * 3 + c]) * 64.0f;
     }
-    __syncthreads();
-    const Blk blk{&sm.px[0][lane]};
+}
 
-    // per-block setup (bc6h.rs:793-819) and encode states (warp 0)
-    if (warp == 0) {
-        Setup su;
-        for (int p = 0; p < 3; p++) {
-            su.bounds[p] = 65535.0f;
-            su.bounds[3 + p] = 0.0f;
+// bc6h_setup (bc6h.rs:793-819) and the state of every encode of the block
+// (compress_bc6h_core's bc6h_test_mode sequence, bc6h.rs:821-860), written
+// to the job rows.
+BCN_DEV void setup_jobs(const Blk& blk, const Work& w, uint32_t gi) {
+    Setup su;
+    for (int p = 0; p < 3; p++) {
+        su.bounds[p] = 65535.0f;
+        su.bounds[3 + p] = 0.0f;
+    }
+    for (int p = 0; p < 3; p++)
+        for (int k = 0; k < 16; k++) {
+            float value = blk(p, k);
+            su.bounds[p] = fminf(su.bounds[p], value);
+            su.bounds[3 + p] = fmaxf(su.bounds[3 + p], value);
         }
-        for (int p = 0; p < 3; p++)
-            for (int k = 0; k < 16; k++) {
-                float value = blk(p, k);
-                su.bounds[p] = fminf(su.bounds[p], value);
-                su.bounds[3 + p] = fmaxf(su.bounds[3 + p], value);
-            }
-        su.max_span = 0.0f;
-        su.max_span_idx = 0;
-        for (int p = 0; p < 3; p++) {
-            float span = su.bounds[3 + p] - su.bounds[p];
-            if (span > su.max_span) {
-                su.max_span_idx = p;
-                su.max_span = span;
-            }
+    su.max_span = 0.0f;
+    su.max_span_idx = 0;
+    for (int p = 0; p < 3; p++) {
+        float span = su.bounds[3 + p] - su.bounds[p];
+        if (span > su.max_span) {
+            su.max_span_idx = p;
+            su.max_span = span;
         }
-        // each encode's state goes straight to shared memory (a local array
-        // indexed by the running count would live in local memory)
-        int n = 0;
-        auto keep = [&](const Job& j) {
-            sm.jmode[n][lane] = j.mode;
-            sm.jepb[n][lane] = j.epb;
-#pragma unroll
-            for (int i = 0; i < 6; i++) sm.jqb[n][i][lane] = j.qb[i];
-            n++;
-        };
-        Job st;
-        st.mode = 0;
-        st.epb = 0;
-        for (int i = 0; i < 6; i++) st.qb[i] = 0;
-        if (S.slow_mode != 0) {
-            // modes 0, 1, 2, 5, 6, 9 (two regions), 10..13 (one region)
-            const uint64_t modes = 0xDCBA965210ull;
-            for (int i = 0; i < 10; i++) {
-                test_mode(su, (int)((modes >> (4 * i)) & 15), 0.0f, st);  // margin 0: always passes
-                keep(st);
-            }
-        } else {
-            if (S.fast_skip_threshold > 0) {
-                test_mode(su, 9, 0.0f, st);
-                if (S.fast_mode != 0) test_mode(su, 1, 1.0f, st);
-                test_mode(su, 6, 1.0f / 1.2f, st);
-                test_mode(su, 5, 1.0f / 1.2f, st);
-                test_mode(su, 0, 1.0f / 1.2f, st);
-                test_mode(su, 2, 1.0f, st);
-                keep(st);
-                if (S.fast_mode == 0) {
-                    test_mode(su, 1, 0.0f, st);
-                    keep(st);
-                }
-            }
-            test_mode(su, 10, 0.0f, st);
-            test_mode(su, 11, 1.0f, st);
-            test_mode(su, 12, 1.0f, st);
-            test_mode(su, 13, 1.0f, st);
+    }
+    int n = 0;
+    auto keep = [&](const Job& j) {
+        w.jobs[(size_t)n * w.npad + gi] = pack_job(j);
+        n++;
+    };
+    Job st;
+    st.mode = 0;
+    st.epb = 0;
+    for (int i = 0; i < 6; i++) st.qb[i] = 0;
+    const BC6HSettingsDev& S = w.S;
+    if (S.slow_mode != 0) {
+        // modes 0, 1, 2, 5, 6, 9 (two regions), 10..13 (one region); margin 0 always passes
+        const uint64_t modes = 0xDCBA965210ull;
+        for (int i = 0; i < 10; i++) {
+            test_mode(su, (int)((modes >> (4 * i)) & 15), 0.0f, st);
+            if (S.fast_skip_threshold > 0 || i >= 6) keep(st);
+        }
+    } else {
+        if (S.fast_skip_threshold > 0) {
+            test_mode(su, 9, 0.0f, st);
+            if (S.fast_mode != 0) test_mode(su, 1, 1.0f, st);
+            test_mode(su, 6, 1.0f / 1.2f, st);
+            test_mode(su, 5, 1.0f / 1.2f, st);
+            test_mode(su, 0, 1.0f / 1.2f, st);
+            test_mode(su, 2, 1.0f, st);
             keep(st);
+            if (S.fast_mode == 0) {
+                test_mode(su, 1, 0.0f, st);
+                keep(st);
+            }
         }
+        test_mode(su, 10, 0.0f, st);
+        test_mode(su, 11, 1.0f, st);
+        test_mode(su, 12, 1.0f, st);
+        test_mode(su, 13, 1.0f, st);
+        keep(st);
     }
+}
 
-    // 2. bounds over the 32 two-region partitions (bc6h.rs:288-302)
-    const bool any2 = P.n2 > 0 && P.k > 0;
-    if (any2) {
-        float full[15];
-        stats_masked<3>(blk, 0xFFFFu, full);
-        for (int part = warp; part < 32; part += NW) {
-            float b12 = pca_bound_split<3>(blk, subset_mask_from_map(kPartitionMap[part], 0), full);
-            sm.keys[part][lane] = part + (int)b12 * 64;
-        }
+// K1: setup + encode states (warp 0), the 32 PCA split bounds of the
+// two-region partitions (bc6h.rs:288-302) over all warps, and the ascending
+// top-k list (partial_sort_list, common.rs:126-140; keys are unique) by the
+// last warp. Also clears the search's argmin keys.
+__global__ void __launch_bounds__(NW * 32, BCN_BC6H_PREP_MINB) bc6h_prep_kernel(Work w) {
+    __shared__ float px[48][NB];
+    __shared__ int keys[32][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    const Blk blk{&px[0][lane]};
+    if (warp == 0) {
+        setup_jobs(blk, w, gi);
+        for (int j = 0; j < P.n2; j++) w.keys[(size_t)j * w.npad + gi] = ~0ull;
+    }
+    if (P.n2 == 0) return;
+    float full[15];
+    stats_masked<3>(blk, 0xFFFFu, full);
+    for (int part = warp; part < 32; part += NW) {
+        float b12 = pca_bound_split<3>(blk, subset_mask_from_map(kPartitionMap[part], 0), full);
+        keys[part][lane] = part + (int)b12 * 64;
     }
     __syncthreads();
-
-    // 3. partial sort (common.rs:126-140)
-    if (any2 && warp == 0) {
+    if (warp == NW - 1) {
         for (int k = 0; k < P.k; k++) {
             int best = INT_MAX, bi = 0;
             for (int q = 0; q < 32; q++) {
-                int v = sm.keys[q][lane];
+                int v = keys[q][lane];
                 if (v < best) {
                     best = v;
                     bi = q;
                 }
             }
-            sm.list[k][lane] = (uint8_t)bi;
-            sm.keys[bi][lane] = INT_MAX;
-        }
-    }
-    __syncthreads();
-
-    // 4. candidates of every two-region encode
-    {
-        float berr[6];
-        int bc[6];
-#pragma unroll
-        for (int j = 0; j < 6; j++) {
-            berr[j] = __int_as_float(0x7f800000);
-            bc[j] = -1;
-        }
-        const int total = any2 ? P.n2 * P.k : 0;
-        for (int item = warp; item < total; item += NW) {
-            int j = item / P.k, c = item - j * P.k;
-            Job st;
-            st.epb = sm.jepb[j][lane];
-#pragma unroll
-            for (int i = 0; i < 6; i++) st.qb[i] = sm.jqb[j][i][lane];
-            int qep[24];
-            uint32_t q0, q1;
-            float err = eval_2p(blk, sm.list[c][lane] & 31, st.epb, st.qb, qep, q0, q1);
-#pragma unroll
-            for (int m = 0; m < 6; m++)
-                if (m == j && err < berr[m]) {
-                    berr[m] = err;
-                    bc[m] = c;
-                }
-        }
-#pragma unroll
-        for (int j = 0; j < 6; j++) {
-            sm.werr[j][warp][lane] = berr[j];
-            sm.wcand[j][warp][lane] = bc[j];
-        }
-    }
-    __syncthreads();
-    if (warp == 0) {
-        for (int j = 0; j < P.n2; j++) {
-            float be = __int_as_float(0x7f800000);
-            int bc = -1;
-            for (int w = 0; w < NW; w++) {
-                float e = sm.werr[j][w][lane];
-                int c = sm.wcand[j][w][lane];
-                if (c >= 0 && (bc < 0 || e < be || (e == be && c < bc))) {
-                    be = e;
-                    bc = c;
-                }
-            }
-            sm.winner[j][lane] = bc;
-            sm.slot_err[j][lane] = be;
-        }
-    }
-    __syncthreads();
-
-    // 5. chains
-    for (int j = warp; j < P.n; j += NW) {
-        Job st;
-        st.mode = sm.jmode[j][lane];
-        st.epb = sm.jepb[j][lane];
-#pragma unroll
-        for (int i = 0; i < 6; i++) st.qb[i] = sm.jqb[j][i][lane];
-        float err = __int_as_float(0x7f800000);
-        uint4 data = make_uint4(0, 0, 0, 0);
-        if (P.kind[j] == 2) {
-            int wc = any2 ? sm.winner[j][lane] : -1;
-            if (wc >= 0) err = refine_code_2p(blk, sm.list[wc][lane] & 31, st, sm.slot_err[j][lane], S.refine_iterations_2p, data);
-        } else {
-            err = encode_1p(blk, st, S.refine_iterations_1p, data);
-        }
-        sm.slot_err[j][lane] = err;
-        sm.slot_data[j][lane] = data;
-    }
-    __syncthreads();
-
-    // 6. select + store
-    if (warp == 0) {
-        float best = __int_as_float(0x7f800000);
-        uint4 data = make_uint4(0, 0, 0, 0);
-        for (int j = 0; j < P.n; j++) {
-            float e = sm.slot_err[j][lane];
-            if (e < best) {
-                best = e;
-                data = sm.slot_data[j][lane];
-            }
-        }
-        uint32_t gi = tile0 + lane;
-        if (gi < nblocks) {
-            uint8_t* o = dst + (size_t)gi * 16;
-            if (((uintptr_t)dst & 15) == 0) {
-                *reinterpret_cast<uint4*>(o) = data;
-            } else {
-                uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
-                o32[0] = data.x;
-                o32[1] = data.y;
-                o32[2] = data.z;
-                o32[3] = data.w;
-            }
+            w.lists[(size_t)k * w.npad + gi] = (uint8_t)bi;
+            keys[bi][lane] = INT_MAX;
         }
     }
 }
 
+// K2: candidate `blockIdx.y * NW + warp` = (two-region encode j, list entry
+// c) for the 32 blocks of the tile (bc6h_enc_2p_part_fast, bc6h.rs:304-324).
+// A candidate counts only with an error below +inf (the reference's running
+// best starts there, bc6h.rs:337); errors are non-negative, so the argmin
+// key's high word orders like the error and the low word keeps the earliest
+// candidate among equal errors, the reference's strict "<" scan.
+__global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_kernel(Work w) {
+    __shared__ float px[48][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    const int item = blockIdx.y * NW + warp;
+    if (item >= P.n2 * P.k || gi >= w.nblocks) return;
+    const int j = item / P.k, c = item - j * P.k;
+    const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
+    const Blk blk{&px[0][lane]};
+    int qep[24];
+    uint32_t q0, q1;
+    const float err = eval_2p(blk, w.lists[(size_t)c * w.npad + gi] & 31, st.epb, st.qb, qep, q0, q1);
+    if (err < __int_as_float(0x7f800000))
+        atomicMin(&w.keys[(size_t)j * w.npad + gi], ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c);
+}
+
+// K3: the winner of two-region encode blockIdx.y, refined (bc6h.rs:355-387);
+// one warp per tile, a private staged tile per warp.
+__global__ void __launch_bounds__(NW * 32, BCN_BC6H_REFINE_MINB) bc6h_refine2_kernel(Work w, uint32_t ntiles) {
+    __shared__ float px[NW][48][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x * NW + warp, gi = tile * NB + lane;
+    if (tile >= ntiles) return;
+    stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    const int j = blockIdx.y;
+    float err = __int_as_float(0x7f800000);
+    const unsigned long long key = w.keys[(size_t)j * w.npad + gi];
+    if (gi < w.nblocks && key != ~0ull) {
+        const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
+        const int part = w.lists[(size_t)(key & 0xFFFFFFFFull) * w.npad + gi] & 31;
+        int qep[16];
+        uint32_t q0, q1;
+        err = refine_2p(Blk{&px[warp][0][lane]}, part, st, __uint_as_float((uint32_t)(key >> 32)),
+                        w.S.refine_iterations_2p, qep, q0, q1);
+        store_pay(w, j, gi, qep, q0, q1, part);
+    }
+    w.slot_err[(size_t)j * w.npad + gi] = err;
+}
+
+// K4: one-region encode n2 + blockIdx.y (bc6h_enc_1p, bc6h.rs:390-412).
+__global__ void __launch_bounds__(NW * 32, BCN_BC6H_ENC1_MINB) bc6h_enc1_kernel(Work w, uint32_t ntiles, int n2) {
+    __shared__ float px[NW][48][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x * NW + warp, gi = tile * NB + lane;
+    if (tile >= ntiles) return;
+    stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    const int j = n2 + blockIdx.y;
+    float err = __int_as_float(0x7f800000);
+    if (gi < w.nblocks) {
+        const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
+        int qep[16];
+        uint32_t q0, q1;
+        err = encode_1p(Blk{&px[warp][0][lane]}, st, w.S.refine_iterations_1p, qep, q0, q1);
+#pragma unroll
+        for (int i = 8; i < 16; i++) qep[i] = 0;
+        store_pay(w, j, gi, qep, q0, q1, 0);
+    }
+    w.slot_err[(size_t)j * w.npad + gi] = err;
+}
+
+// K5: the reference's sequential strict comparisons over the encodes, in
+// order (self.best_err starts at +inf), then the coding of the winner alone
+// (coding depends only on the winner's endpoints, indices, partition and
+// mode; the reference codes on every improvement, bc6h.rs:383-386, 407-411,
+// and keeps the last) and the block's 128-bit store. A block no encode
+// improved stays all zero, as the reference's data array.
+__global__ void __launch_bounds__(128) bc6h_select_kernel(Work w, int n, int n2) {
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= w.nblocks) return;
+    float best = __int_as_float(0x7f800000);
+    int win = -1;
+    for (int j = 0; j < n; j++) {
+        const float e = w.slot_err[(size_t)j * w.npad + gi];
+        if (e < best) {
+            best = e;
+            win = j;
+        }
+    }
+    uint4 data = make_uint4(0, 0, 0, 0);
+    if (win >= 0) {
+        int qep[24];
+        uint32_t q0, q1;
+        int part;
+        load_pay(w, win, gi, qep, q0, q1, part);
+        const int mode = (int)(w.jobs[(size_t)win * w.npad + gi].x & 0xFFu);
+        data = win < n2 ? code_2p(qep, q0, q1, part, mode) : code_1p(qep, q0, q1, mode);
+    }
+    uint8_t* o = w.dst + (size_t)gi * 16;
+    if (((uintptr_t)w.dst & 15) == 0) {
+        *reinterpret_cast<uint4*>(o) = data;
+    } else {
+        uint32_t* o32 = reinterpret_cast<uint32_t*>(o);
+        o32[0] = data.x;
+        o32[1] = data.y;
+        o32[2] = data.z;
+        o32[3] = data.w;
+    }
+}
+
+// Scratch layout, each array 256-byte aligned.
+struct Layout {
+    size_t jobs, lists, keys, slot_err, slot_pay, total;
+};
+static Layout layout(uint32_t npad, const Plan& P) {
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    Layout L;
+    L.jobs = 0;
+    L.lists = up(L.jobs + (size_t)P.n * npad * sizeof(uint4));
+    L.keys = up(L.lists + (size_t)(P.k > 0 ? P.k : 1) * npad);
+    L.slot_err = up(L.keys + (size_t)(P.n2 > 0 ? P.n2 : 1) * npad * sizeof(unsigned long long));
+    L.slot_pay = up(L.slot_err + (size_t)P.n * npad * sizeof(float));
+    L.total = up(L.slot_pay + (size_t)P.n * 3 * npad * sizeof(uint4));
+    return L;
+}
+
 }  // namespace bc6h
 
-void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,
-                        uint8_t* dst, const BC6HSettingsDev& settings, cudaStream_t s) {
-    uint32_t n = bw * bh;
-    if (n == 0) return;
-    uint32_t grid = (n + bptc::NB - 1) / bptc::NB;
-    bc6h::bc6h_encode_kernel<<<grid, bc6h::NW * 32, 0, s>>>((const uint8_t*)src, stride_bytes, source_format, bw, n,
-                                                            dst, settings);
+size_t bc6h_scratch_bytes(uint32_t nblocks, const BC6HSettingsDev& settings) {
+    const uint32_t npad = (nblocks + bptc::NB - 1) / bptc::NB * bptc::NB;
+    return bc6h::layout(npad, bc6h::make_plan(settings)).total;
+}
+
+namespace bc6h {
+// The side stream of launch_bc6h_encode with its fork and join events, per
+// host thread, created on first use for the current device.
+struct SideStream {
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    int device = -1;
+    void release() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (st) cudaStreamDestroy(st);
+        fork = join = nullptr;
+        st = nullptr;
+        device = -1;
+    }
+    ~SideStream() { release(); }
+    cudaError_t get() {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess || dev == device) return e;
+        release();
+        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming)) != cudaSuccess) return e;
+        device = dev;
+        return cudaSuccess;
+    }
+};
+static thread_local SideStream t_side;
+}  // namespace bc6h
+
+// prep on `s`; then the one-region encodes (they need only the encode
+// states) on a side stream forked from `s`, while `s` runs the two-region
+// search and refinement; joined before the selection. While `s` captures a
+// graph, the side stream is used only if this thread made it earlier for
+// the device (a stream is not created during a capture); otherwise every
+// launch stays on `s`.
+cudaError_t launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,
+                               uint8_t* dst, const BC6HSettingsDev& settings, void* scratch, cudaStream_t s) {
+    using namespace bc6h;
+    const uint32_t n = bw * bh;
+    if (n == 0) return cudaSuccess;
+    const uint32_t ntiles = (n + NB - 1) / NB, npad = ntiles * NB;
+    const Plan P = make_plan(settings);
+    const Layout L = layout(npad, P);
+    uint8_t* base = (uint8_t*)scratch;
+    Work w;
+    w.src = (const uint8_t*)src;
+    w.stride = stride_bytes;
+    w.source_format = source_format;
+    w.aligned = ((uintptr_t)src % 16 == 0) && (stride_bytes % 16 == 0);
+    w.bw = bw;
+    w.nblocks = n;
+    w.npad = npad;
+    w.dst = dst;
+    w.jobs = (uint4*)(base + L.jobs);
+    w.lists = base + L.lists;
+    w.keys = (unsigned long long*)(base + L.keys);
+    w.slot_err = (float*)(base + L.slot_err);
+    w.slot_pay = (uint4*)(base + L.slot_pay);
+    w.S = settings;
+    cudaError_t e;
+    bc6h_prep_kernel<<<ntiles, NW * 32, 0, s>>>(w);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaStream_t s1 = s;
+    if (P.n2 > 0 && P.n > P.n2) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if ((e = cudaStreamIsCapturing(s, &cs)) != cudaSuccess) return e;
+        int dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if (cs == cudaStreamCaptureStatusNone || t_side.device == dev) {
+            if ((e = t_side.get()) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(t_side.fork, s)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(t_side.st, t_side.fork, 0)) != cudaSuccess) return e;
+            s1 = t_side.st;
+        }
+    }
+    if (P.n > P.n2)
+        bc6h_enc1_kernel<<<dim3((ntiles + NW - 1) / NW, (uint32_t)(P.n - P.n2)), NW * 32, 0, s1>>>(w, ntiles, P.n2);
+    if (P.n2 > 0) {
+        const uint32_t groups = (uint32_t)(P.n2 * P.k + NW - 1) / NW;
+        bc6h_search_kernel<<<dim3(ntiles, groups), NW * 32, 0, s>>>(w);
+        bc6h_refine2_kernel<<<dim3((ntiles + NW - 1) / NW, (uint32_t)P.n2), NW * 32, 0, s>>>(w, ntiles);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (s1 != s) {
+        if ((e = cudaEventRecord(t_side.join, s1)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s, t_side.join, 0)) != cudaSuccess) return e;
+    }
+    bc6h_select_kernel<<<(n + 127) / 128, 128, 0, s>>>(w, P.n, P.n2);
+    return cudaGetLastError();
 }
 
 }  // namespace bcn

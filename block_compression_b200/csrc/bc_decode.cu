@@ -737,3 +737,94 @@ void launch_decode_blocks(int kind, const uint8_t* blocks, size_t nblocks, void*
 }
 
 }  // namespace bcn
+
+// ---- BC6H quality against the RGBA16F source ------------------------------------
+//
+// Per block: the decoded texels (unsigned decoder, the image drivers' form)
+// against the source's f16 values, both widened exactly to f64:
+//   squared RGB error   sum over texels and R, G, B of (decoded - source)^2
+//   log-luminance error sum over texels of (log2 L(decoded) - log2 L(source))^2,
+//                       L = 0.2126 R + 0.7152 G + 0.0722 B (Rec. 709), floored
+//                       at 2^-24 (the smallest f16 step) so black texels stay
+//                       finite.
+// A fixed grid reduces blocks to per-CTA partials, and one CTA adds the
+// partials in CTA order, so the sums do not depend on scheduling.
+namespace bcn {
+
+constexpr int kErrThreads = 128;
+constexpr int kErrCtas = 148 * 8;
+
+BCN_DEV double half_to_double(uint32_t h) { return (double)__half2float(__ushort_as_half((uint16_t)h)); }
+
+BCN_DEV double log2_lum(double r, double g, double b) {
+    double l = 0.2126 * r + 0.7152 * g + 0.0722 * b;
+    return log2(l > 0x1p-24 ? l : 0x1p-24);
+}
+
+__global__ void __launch_bounds__(kErrThreads) bc6h_error_partial_kernel(const uint8_t* __restrict__ blocks, uint32_t bw,
+                                                                         uint32_t nblocks, const uint16_t* __restrict__ src,
+                                                                         size_t src_pitch, double* __restrict__ block_sse,
+                                                                         double* __restrict__ partial) {
+    __shared__ double red[kErrThreads / 32][2];
+    double acc_sse = 0.0, acc_log = 0.0;
+    for (uint32_t i = blockIdx.x * kErrThreads + threadIdx.x; i < nblocks; i += gridDim.x * kErrThreads) {
+        const uint8_t* b = blocks + (size_t)i * 16;
+        uint64_t lo = 0, hi = 0;
+        for (int j = 0; j < 8; j++) lo |= (uint64_t)b[j] << (8 * j);
+        for (int j = 0; j < 8; j++) hi |= (uint64_t)b[8 + j] << (8 * j);
+        uint32_t h[24];
+        decode_bc6h_block<false>(lo, hi, h);
+        const uint32_t by = i / bw, bx = i - by * bw;
+        double sse = 0.0, lg = 0.0;
+        for (int k = 0; k < 16; k++) {
+            const uint16_t* s = src + (size_t)(by * 4 + k / 4) * src_pitch + (size_t)(bx * 4 + k % 4) * 4;
+            double d[3], o[3];
+            for (int c = 0; c < 3; c++) {
+                const int e = k * 3 + c;
+                d[c] = half_to_double(h[e >> 1] >> (16 * (e & 1)));
+                o[c] = half_to_double(s[c]);
+                sse += (d[c] - o[c]) * (d[c] - o[c]);
+            }
+            const double t = log2_lum(d[0], d[1], d[2]) - log2_lum(o[0], o[1], o[2]);
+            lg += t * t;
+        }
+        if (block_sse) block_sse[i] = sse;
+        acc_sse += sse;
+        acc_log += lg;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_sse += __shfl_down_sync(0xFFFFFFFFu, acc_sse, o);
+        acc_log += __shfl_down_sync(0xFFFFFFFFu, acc_log, o);
+    }
+    if (lane == 0) {
+        red[warp][0] = acc_sse;
+        red[warp][1] = acc_log;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double v = 0.0;
+        for (int w = 0; w < kErrThreads / 32; w++) v += red[w][threadIdx.x];
+        partial[(size_t)blockIdx.x * 2 + threadIdx.x] = v;
+    }
+}
+
+__global__ void bc6h_error_final_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+    if (threadIdx.x < 2) {
+        double v = 0.0;
+        for (int i = 0; i < n; i++) v += partial[(size_t)i * 2 + threadIdx.x];
+        out[threadIdx.x] = v;
+    }
+}
+
+cudaError_t launch_bc6h_error(const uint8_t* blocks, uint32_t bw, uint32_t bh, const uint16_t* src, size_t src_pitch,
+                              double* sums, double* block_sse, double* partial, cudaStream_t s) {
+    const uint32_t n = bw * bh;
+    bc6h_error_partial_kernel<<<kErrCtas, kErrThreads, 0, s>>>(blocks, bw, n, src, src_pitch, block_sse, partial);
+    bc6h_error_final_kernel<<<1, 32, 0, s>>>(partial, kErrCtas, sums);
+    return cudaGetLastError();
+}
+
+size_t bc6h_error_partial_bytes() { return sizeof(double) * 2 * kErrCtas; }
+
+}  // namespace bcn

@@ -68,9 +68,12 @@ cudaError_t launch_bc7_batch(const TaskDesc* tasks_dev, const uint32_t* tile_tas
 cudaError_t launch_bc15_batch(const TaskDesc* tasks_dev, const uint32_t* tile_task_dev, uint32_t ntiles,
                               uint32_t* counter_dev, int threads, int ctas, int tiles_per_claim, cudaStream_t s);
 void launch_bc7_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, uint8_t* out, size_t pitch, cudaStream_t s);
-// stride in bytes of the source rows (RGBA16F: 8 bytes per pixel; RGBA8: 4).
-void launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,
-                        uint8_t* dst, const BC6HSettingsDev& settings, cudaStream_t s);
+// BC6H runs as a pipeline of kernels exchanging per-block state through
+// `scratch` (device memory of at least bc6h_scratch_bytes()). stride in bytes
+// of the source rows (RGBA16F: 8 bytes per pixel; RGBA8: 4).
+size_t bc6h_scratch_bytes(uint32_t nblocks, const BC6HSettingsDev& settings);
+cudaError_t launch_bc6h_encode(const void* src, size_t stride_bytes, int source_format, uint32_t bw, uint32_t bh,
+                               uint8_t* dst, const BC6HSettingsDev& settings, void* scratch, cudaStream_t s);
 // out_format: 0 RGBA8 (sRGB-encoded), 1 RGBA16F (RGB triplets in RGBA rows),
 // 2 RGBA32F (same layout); pitch in output elements.
 void launch_bc6h_decode(const uint8_t* blocks, uint32_t bw, uint32_t bh, void* out, size_t pitch, int out_format,
@@ -88,6 +91,14 @@ enum BlockKind {
 // reference's element order.
 void launch_decode_blocks(int kind, const uint8_t* blocks, size_t nblocks, void* out, size_t pitch,
                           size_t out_block_stride, cudaStream_t s);
+
+// BC6H quality of `blocks` against the RGBA16F source (pitch in f16
+// elements): sums[0] = squared RGB error, sums[1] = squared log2-luminance
+// error, both in f64 over the image; block_sse (optional) the squared RGB
+// error per block. partial: device scratch of bc6h_error_partial_bytes().
+cudaError_t launch_bc6h_error(const uint8_t* blocks, uint32_t bw, uint32_t bh, const uint16_t* src, size_t src_pitch,
+                              double* sums, double* block_sse, double* partial, cudaStream_t s);
+size_t bc6h_error_partial_bytes();
 
 // Settings check shared by every BC7 entry point (BC_OK or a BC_ERR_* code),
 // and the per-thread record behind bc_last_cuda_error().

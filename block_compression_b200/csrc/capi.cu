@@ -118,7 +118,16 @@ static int enqueue_encode(int variant, const void* settings, const uint8_t* src,
         case BC_BC6H: {
             int rc = upload_bc6h_tables();
             if (rc != BC_OK) return rc;
-            launch_bc6h_encode(src, stride, bc6h_source, bw, bh, dst, *(const BC6HSettingsDev*)settings, s);
+            const BC6HSettingsDev& s6 = *(const BC6HSettingsDev*)settings;
+            cudaMemPool_t pool;
+            rc = scratch_pool(&pool);
+            if (rc != BC_OK) return rc;
+            void* scratch = nullptr;
+            BC_CUDA(cudaMallocFromPoolAsync(&scratch, bc6h_scratch_bytes(bw * bh, s6), pool, s));
+            cudaError_t e = launch_bc6h_encode(src, stride, bc6h_source, bw, bh, dst, s6, scratch, s);
+            cudaError_t f = cudaFreeAsync(scratch, s);
+            BC_CUDA(e);
+            BC_CUDA(f);
             break;
         }
         default:

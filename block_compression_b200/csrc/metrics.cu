@@ -123,3 +123,32 @@ extern "C" int bc_image_sse_rgba8_device(const uint8_t* a, size_t pitch_a, const
     }
     return BC_OK;
 }
+
+extern "C" int bc_bc6h_error_device(const uint16_t* src_dev, size_t src_len_elems, size_t src_stride_elems,
+                                    const uint8_t* blocks_dev, size_t blocks_len, uint32_t width, uint32_t height,
+                                    double* sums_out, double* block_sse_out, void* stream) {
+    if (!src_dev || !blocks_dev || !sums_out) return BC_ERR_NULL;
+    if (width % 4 || height % 4) return BC_ERR_DIMS;
+    const uint32_t bw = width / 4, bh = height / 4;
+    if (blocks_len < (size_t)bw * bh * 16) return BC_ERR_SRC_SIZE;
+    if (src_stride_elems < (size_t)width * 4) return BC_ERR_SRC_SIZE;
+    if (height > 0 && src_len_elems < (size_t)(height - 1) * src_stride_elems + (size_t)width * 4)
+        return BC_ERR_SRC_SIZE;
+    if ((uintptr_t)sums_out % 8 || (uintptr_t)block_sse_out % 8 || (uintptr_t)src_dev % 2) return BC_ERR_SRC_SIZE;
+    if (bw == 0 || bh == 0) return BC_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    double* partial = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&partial, bc6h_error_partial_bytes(), s);
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return BC_ERR_CUDA;
+    }
+    e = launch_bc6h_error(blocks_dev, bw, bh, src_dev, src_stride_elems, sums_out, block_sse_out, partial, s);
+    cudaError_t f = cudaFreeAsync(partial, s);
+    if (e == cudaSuccess) e = f;
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return BC_ERR_CUDA;
+    }
+    return BC_OK;
+}

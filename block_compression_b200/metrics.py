@@ -61,3 +61,34 @@ def calculate_image_metrics_rgba8(original, compressed, width, height, channels=
     Returns a PsnrResult (synchronises to read the four sums)."""
     sse = image_sse_rgba8(original, compressed, width, height, channels)
     return PsnrResult(sse.cpu().tolist(), float(width * height), channels)
+
+
+def bc6h_error(src, blocks, width, height, stride=None, block_sse=None, stream=None):
+    """FP64 quality of BC6H `blocks` against their RGBA16F source `src` (CUDA
+    buffers; stride in f16 elements, default width * 4). Returns a CUDA
+    float64 tensor of 2: the squared RGB error and the squared log2-luminance
+    error summed over the image; `block_sse` (CUDA float64, one per block)
+    receives each block's squared RGB error. Stream-ordered."""
+    import torch
+
+    vs, vb = _buffers.view(src), _buffers.view(blocks)
+    if not (vs.cuda and vb.cuda):
+        raise ValueError("bc6h_error takes CUDA buffers")
+    out = torch.zeros(2, dtype=torch.float64, device=blocks.device)
+    bp = None
+    if block_sse is not None:
+        bp = _buffers.view(block_sse, writable=True)
+        if bp.nbytes < (width // 4) * (height // 4) * 8:
+            check("bc_bc6h_error_device", -2)
+    s = stream if stream is not None else _buffers.current_stream_ptr()
+    check("bc_bc6h_error_device",
+          lib.bc_bc6h_error_device(vs.ptr, vs.nbytes // 2, stride or width * 4, vb.ptr, vb.nbytes, width, height,
+                                   out.data_ptr(), bp.ptr if bp is not None else None, s))
+    return out
+
+
+def log_luminance_rmse(src, blocks, width, height, stride=None):
+    """Root-mean-square error of log2 luminance (Rec. 709 weights) of the
+    decoded BC6H image against its RGBA16F source (synchronises)."""
+    sums = bc6h_error(src, blocks, width, height, stride).cpu().tolist()
+    return math.sqrt(sums[1] / (width * height))

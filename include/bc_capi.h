@@ -381,6 +381,23 @@ int bc_image_sse_rgba8_device(const uint8_t* a, size_t pitch_a, const uint8_t* b
                               uint32_t width, uint32_t height, uint32_t channels, double* sse_out,
                               void* stream);
 
+/* BC6H quality of encoded blocks against their RGBA16F source (the HDR
+ * metric of the BC6H workload; the reference's own tests measure BC6H only
+ * after an sRGB round trip to RGBA8). Both images are widened exactly to
+ * f64; per texel the decoded RGB (the unsigned decoder of the image drivers,
+ * src/decode.rs:397) is compared with the source RGB:
+ *   sums_out[0] = sum over texels and R, G, B of (decoded - source)^2,
+ *   sums_out[1] = sum over texels of (log2 L(decoded) - log2 L(source))^2,
+ *                 L = 0.2126 R + 0.7152 G + 0.0722 B, floored at 2^-24;
+ * the log-luminance RMSE is sqrt(sums_out[1] / (width * height)).
+ * block_sse_out (optional, one double per block, row-major) receives each
+ * block's squared RGB error. src_len_elems and src_stride_elems in f16
+ * elements; device buffers; stream-ordered. The sums are added in a fixed
+ * order. */
+int bc_bc6h_error_device(const uint16_t* src_dev, size_t src_len_elems, size_t src_stride_elems,
+                         const uint8_t* blocks_dev, size_t blocks_len, uint32_t width, uint32_t height,
+                         double* sums_out, double* block_sse_out, void* stream);
+
 /* ---- DDS container (the reference CLI's output, compressor/src/main.rs:313-353)
  * bc_dds_header writes the 148-byte header of a DX10-extended DDS file for one
  * 2D texture: "DDS " + DDS_HEADER + DDS_HEADER_DXT10, straight alpha, the
