@@ -93,6 +93,9 @@ def _load():
         "bc_dds_header": ([I, U32, U32, U32, I, P, S], I),
         "bc_dds_dxgi_format": ([I, I], U32),
         "bc_last_cuda_error": ([], I),
+        "bc_check_enabled": ([], I),
+        "bc_check_read": ([P], I),
+        "bc_check_selftest": ([ctypes.c_uint64, ctypes.c_uint64, P], I),
         "bc_version": ([], ctypes.c_char_p),
     }
     for name, (args, res) in sig.items():

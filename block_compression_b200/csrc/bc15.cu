@@ -12,6 +12,7 @@
 #include "bc_common.cuh"
 #include "bc_kernels.h"
 #include "bc1_block.cuh"
+#include "bc_check.cuh"
 
 namespace bcn {
 
@@ -301,12 +302,13 @@ __global__ void __launch_bounds__(128) bc15_encode_kernel(const uint8_t* __restr
     uint32_t n = bw * bh;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t by = i / bw, bx = i - by * bw;
+        if (!BCN_GUARD(by, bh, CHECK_BC15_LOAD) || !BCN_GUARD(bx, bw, CHECK_BC15_LOAD)) continue;
         Px16 px;
         load_rgba8<ALIGNED_SRC>(src, stride, bx, by, px);
         uint32_t w[4];
         encode_bc15_block(VARIANT, px, w);
         constexpr int words = (VARIANT == BC_BC1 || VARIANT == BC_BC4) ? 2 : 4;
-        store_block<ALIGNED_DST>(dst + (size_t)i * (words * 4), w, words);
+        if (BCN_GUARD(i, n, CHECK_BC15_STORE)) store_block<ALIGNED_DST>(dst + (size_t)i * (words * 4), w, words);
     }
 }
 
@@ -367,6 +369,7 @@ __global__ void __launch_bounds__(128) bc15_decode_kernel(const uint8_t* __restr
         }
         uint32_t px[16];
         decode_bc15_rgba8(VARIANT, w, px);
+        if (!BCN_GUARD(by, bh, CHECK_DECODE_STORE) || !BCN_GUARD(bx, bw, CHECK_DECODE_STORE)) continue;
 #pragma unroll
         for (int y = 0; y < 4; y++) {
             uint8_t* row = out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16;
@@ -484,4 +487,8 @@ void launch_bc15_decode(int variant, const uint8_t* blocks, uint32_t bw, uint32_
     }
 }
 
+}  // namespace bcn
+
+namespace bcn {
+cudaError_t check_take_bc15(unsigned long long out[3]) { return check_record_take(out); }
 }  // namespace bcn

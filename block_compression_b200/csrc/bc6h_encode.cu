@@ -34,6 +34,7 @@
 #include "bc_common.cuh"
 #include "bc_kernels.h"
 #include "bptc_math.cuh"
+#include "bc_check.cuh"
 
 namespace bcn {
 
@@ -517,6 +518,12 @@ struct Work {
     BC6HSettingsDev S;
 };
 
+// Row `row` of a scratch array with `rows` rows, at block gi: whether the
+// guarded index is inside the array (always true outside check builds).
+BCN_DEV bool scratch_ok(const Work& w, int row, int rows, uint32_t gi) {
+    return BCN_GUARD(row, rows, CHECK_BC6H_SCRATCH) && BCN_GUARD(gi, w.npad, CHECK_BC6H_SCRATCH);
+}
+
 // An encode's result in three 16-byte rows: the 16 endpoint values as 16-bit
 // pairs (BC6H endpoints are below 2^16), then the indices and the partition.
 BCN_DEV void store_pay(const Work& w, int j, uint32_t gi, const int qep[16], uint32_t q0, uint32_t q1, int part) {
@@ -553,7 +560,7 @@ BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, 
         float v[12];
 #pragma unroll
         for (int i = 0; i < 12; i++) v[i] = 0.0f;
-        if (gi < w.nblocks) {
+        if (gi < w.nblocks && BCN_GUARD(gi / w.bw * 4 + y, (w.nblocks + w.bw - 1) / w.bw * 4, CHECK_BC6H_STAGE)) {
             const uint32_t by = gi / w.bw, bx = gi - by * w.bw;
             const uint8_t* row = w.src + (size_t)(by * 4 + y) * w.stride;
             if (w.source_format == BC6H_SRC_RGBA16F) {
@@ -614,8 +621,9 @@ BCN_DEV void setup_jobs(const Blk& blk, const Work& w, uint32_t gi) {
         }
     }
     int n = 0;
+    const int njobs = make_plan(w.S).n;
     auto keep = [&](const Job& j) {
-        w.jobs[(size_t)n * w.npad + gi] = pack_job(j);
+        if (scratch_ok(w, n, njobs, gi)) w.jobs[(size_t)n * w.npad + gi] = pack_job(j);
         n++;
     };
     Job st;
@@ -667,7 +675,8 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_PREP_MINB) bc6h_prep_kernel(
     const Blk blk{&px[0][lane]};
     if (warp == 0) {
         setup_jobs(blk, w, gi);
-        for (int j = 0; j < P.n2; j++) w.keys[(size_t)j * w.npad + gi] = ~0ull;
+        for (int j = 0; j < P.n2; j++)
+            if (scratch_ok(w, j, P.n2, gi)) w.keys[(size_t)j * w.npad + gi] = ~0ull;
     }
     if (P.n2 == 0) return;
     float full[15];
@@ -687,7 +696,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_PREP_MINB) bc6h_prep_kernel(
                     bi = q;
                 }
             }
-            w.lists[(size_t)k * w.npad + gi] = (uint8_t)bi;
+            if (scratch_ok(w, k, P.k, gi)) w.lists[(size_t)k * w.npad + gi] = (uint8_t)bi;
             keys[bi][lane] = INT_MAX;
         }
     }
@@ -709,6 +718,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_ker
     const int item = blockIdx.y * NW + warp;
     if (item >= P.n2 * P.k || gi >= w.nblocks) return;
     const int j = item / P.k, c = item - j * P.k;
+    if (!scratch_ok(w, j, P.n2, gi) || !scratch_ok(w, c, P.k, gi)) return;
     const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
     const Blk blk{&px[0][lane]};
     int qep[24];
@@ -728,9 +738,11 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_REFINE_MINB) bc6h_refine2_ke
     stage_tile(px[warp], w, tile, lane, 32);
     __syncwarp();
     const int j = blockIdx.y;
+    const Plan P = make_plan(w.S);
+    if (!scratch_ok(w, j, P.n2, gi)) return;
     float err = __int_as_float(0x7f800000);
     const unsigned long long key = w.keys[(size_t)j * w.npad + gi];
-    if (gi < w.nblocks && key != ~0ull) {
+    if (gi < w.nblocks && key != ~0ull && scratch_ok(w, (int)(key & 0xFFFFFFFFull), P.k, gi)) {
         const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
         const int part = w.lists[(size_t)(key & 0xFFFFFFFFull) * w.npad + gi] & 31;
         int qep[16];
@@ -751,6 +763,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_ENC1_MINB) bc6h_enc1_kernel(
     stage_tile(px[warp], w, tile, lane, 32);
     __syncwarp();
     const int j = n2 + blockIdx.y;
+    if (!scratch_ok(w, j, make_plan(w.S).n, gi)) return;
     float err = __int_as_float(0x7f800000);
     if (gi < w.nblocks) {
         const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
@@ -776,7 +789,7 @@ __global__ void __launch_bounds__(128) bc6h_select_kernel(Work w, int n, int n2)
     float best = __int_as_float(0x7f800000);
     int win = -1;
     for (int j = 0; j < n; j++) {
-        const float e = w.slot_err[(size_t)j * w.npad + gi];
+        const float e = scratch_ok(w, j, n, gi) ? w.slot_err[(size_t)j * w.npad + gi] : __int_as_float(0x7f800000);
         if (e < best) {
             best = e;
             win = j;
@@ -791,6 +804,7 @@ __global__ void __launch_bounds__(128) bc6h_select_kernel(Work w, int n, int n2)
         const int mode = (int)(w.jobs[(size_t)win * w.npad + gi].x & 0xFFu);
         data = win < n2 ? code_2p(qep, q0, q1, part, mode) : code_1p(qep, q0, q1, mode);
     }
+    if (!BCN_GUARD(gi, w.nblocks, CHECK_BC6H_STORE)) return;
     uint8_t* o = w.dst + (size_t)gi * 16;
     if (((uintptr_t)w.dst & 15) == 0) {
         *reinterpret_cast<uint4*>(o) = data;
@@ -820,6 +834,8 @@ static Layout layout(uint32_t npad, const Plan& P) {
 }
 
 }  // namespace bc6h
+
+cudaError_t check_take_bc6h(unsigned long long out[3]) { return check_record_take(out); }
 
 size_t bc6h_scratch_bytes(uint32_t nblocks, const BC6HSettingsDev& settings) {
     const uint32_t npad = (nblocks + bptc::NB - 1) / bptc::NB * bptc::NB;

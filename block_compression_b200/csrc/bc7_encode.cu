@@ -37,6 +37,7 @@
 #include "bc_kernels.h"
 #include "bptc_math.cuh"
 #include "bc7_device.cuh"
+#include "bc_check.cuh"
 
 // Minimum resident CTAs per SM requested from the register allocator.
 #ifndef BCN_MODE45_MINB
@@ -161,6 +162,13 @@ BCN_DEV TileLoc tile_loc(const Work& w, uint32_t tile) {
     return t;
 }
 
+// Row `row` of a scratch array with `rows` rows, at block gi: whether the
+// guarded index is inside the array (always true outside check builds).
+BCN_DEV bool scratch_ok(const Work& w, int row, int rows, uint32_t gi) {
+    return BCN_GUARD(row, rows, CHECK_BC7_SCRATCH) && BCN_GUARD(gi, w.npad, CHECK_BC7_SCRATCH);
+}
+BCN_DEV int nslots_of(const Plan& P) { return 5 + P.n45_4 + P.n45_5 + 1; }
+
 // Stages the 32 blocks of `tile` into px (planar f32, lane-strided) with
 // threads tid = 0..nt-1 (128-bit loads: the 4 rows of 32 neighbouring blocks
 // are 4 contiguous 512-byte spans).
@@ -172,6 +180,10 @@ BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, 
         uint32_t v[4] = {0, 0, 0, 0};
         if (gi < L.nblocks) {
             uint32_t by = gi / L.bw, bx = gi - by * L.bw;
+            // the image's rows and block columns
+            if (!BCN_GUARD(by * 4 + y, (L.nblocks + L.bw - 1) / L.bw * 4, CHECK_BC7_STAGE) ||
+                !BCN_GUARD(bx, L.bw, CHECK_BC7_STAGE))
+                continue;
             const uint8_t* row = L.src + (size_t)(by * 4 + y) * L.stride + (size_t)bx * 16;
             if (L.aligned) {
                 uint4 q = __ldg(reinterpret_cast<const uint4*>(row));
@@ -275,7 +287,8 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
             for (int i = 0; i < 8; i++) m = min(m, keys[set][8 * bg + i][lane]);
 #pragma unroll
             for (int g = 0; g < 8; g++) gm[g] = g == bg ? m : gm[g];
-            w.lists[(size_t)(set == 0 ? k : P.k_a + k) * w.npad + gi] = (uint8_t)bi;
+            const int row = set == 0 ? k : P.k_a + k;
+            if (scratch_ok(w, row, P.k_a + P.k_b, gi)) w.lists[(size_t)row * w.npad + gi] = (uint8_t)bi;
         }
     }
 }
@@ -283,7 +296,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
 BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
     if (mi <= 1) return c + 64;  // modes 0 and 2: partitions 0..count-1 of the 3-subset table
     int row = (mi == 4 && P.bounds_b) ? P.k_a + c : c;
-    return w.lists[(size_t)row * w.npad + gi];
+    return scratch_ok(w, row, P.k_a + P.k_b, gi) ? w.lists[(size_t)row * w.npad + gi] : 0;
 }
 
 // K2: every partition candidate of one mode (bc7.rs:517-569). Grid: (tile,
@@ -326,7 +339,7 @@ __global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_S
     if (warp == 0) {
         unsigned long long k = best[0][lane];
         for (int i = 1; i < NW; i++) k = min(k, best[i][lane]);
-        if (k != ~0ull) atomicMin(&w.keys[(size_t)mi * w.npad + gi], k);
+        if (k != ~0ull && scratch_ok(w, mi, 5, gi)) atomicMin(&w.keys[(size_t)mi * w.npad + gi], k);
     }
 }
 
@@ -344,7 +357,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_REFINE_MINB) bc7_refine_kernel(Wo
     const uint32_t gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
     const Blk blk{&px[warp][0][lane]};
-    unsigned long long key = w.keys[(size_t)mi * w.npad + gi];
+    unsigned long long key = scratch_ok(w, mi, 5, gi) ? w.keys[(size_t)mi * w.npad + gi] : ~0ull;
     float err = __int_as_float(0x7f800000);
     uint4 data = make_uint4(0, 0, 0, 0);
     if (key != ~0ull && tile_loc(w, tile).valid(lane)) {
@@ -354,8 +367,10 @@ __global__ void __launch_bounds__(NW * 32, BCN_REFINE_MINB) bc7_refine_kernel(Wo
         err = refine_and_code<MODE>(blk, kPartitionMap, part_of(w, mi, c, gi, P), e0, iters,
                                     opaque_err(blk, w.S.channels), data);
     }
-    w.slot_err[(size_t)mi * w.npad + gi] = err;
-    w.slot_data[(size_t)mi * w.npad + gi] = data;
+    if (scratch_ok(w, mi, nslots_of(P), gi)) {
+        w.slot_err[(size_t)mi * w.npad + gi] = err;
+        w.slot_data[(size_t)mi * w.npad + gi] = data;
+    }
 }
 
 // K4: mode 4 / mode 5 rotation candidates (bc7.rs:657-760); mode 4 runs one
@@ -383,8 +398,10 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Wo
     // candidate order of the reference: mode 4 (rotation, swap 0), (rotation,
     // swap 1), ... then mode 5 rotations
     int slot = 5 + (MODE == 4 ? 2 * r + SWAP : P.n45_4 + r);
-    w.slot_err[(size_t)slot * w.npad + gi] = err;
-    w.slot_data[(size_t)slot * w.npad + gi] = data;
+    if (scratch_ok(w, slot, nslots_of(P), gi)) {
+        w.slot_err[(size_t)slot * w.npad + gi] = err;
+        w.slot_data[(size_t)slot * w.npad + gi] = data;
+    }
 }
 
 // K5: mode 6 (bc7.rs:762-817), one warp per tile.
@@ -402,8 +419,10 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE6_MINB) bc7_mode6_kernel(Work
     uint4 data;
     float err = mode6<CH>(blk, w.S.refine_iterations[6], data);
     int slot = 5 + P.n45_4 + P.n45_5;
-    w.slot_err[(size_t)slot * w.npad + gi] = err;
-    w.slot_data[(size_t)slot * w.npad + gi] = data;
+    if (scratch_ok(w, slot, nslots_of(P), gi)) {
+        w.slot_err[(size_t)slot * w.npad + gi] = err;
+        w.slot_data[(size_t)slot * w.npad + gi] = data;
+    }
 }
 
 // K6: the reference keeps a candidate only when its error is strictly below
@@ -420,9 +439,13 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w, uint32_t ntiles
     const Plan P = make_plan(w.S);
     float best = __int_as_float(0x7f800000);
     int win = -1;
+    const int nslots = nslots_of(P);
+    auto slot_err = [&](int s) {
+        return scratch_ok(w, s, nslots, gi) ? w.slot_err[(size_t)s * w.npad + gi] : __int_as_float(0x7f800000);
+    };
     for (int s = 0; s < 5; s++)
         if (P.count[s] > 0) {
-            float e = w.slot_err[(size_t)s * w.npad + gi];
+            float e = slot_err(s);
             if (e < best) {
                 best = e;
                 win = s;
@@ -430,7 +453,7 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w, uint32_t ntiles
         }
     const int n45 = P.n45_4 + P.n45_5;
     for (int s = 5; s < 5 + n45; s++) {
-        float e = w.slot_err[(size_t)s * w.npad + gi];
+        float e = slot_err(s);
         if (e < best) {
             best = e;
             win = s;
@@ -438,13 +461,15 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w, uint32_t ntiles
     }
     if (P.run6) {
         int s = 5 + n45;
-        float e = w.slot_err[(size_t)s * w.npad + gi];
+        float e = slot_err(s);
         if (e < best) {
             best = e;
             win = s;
         }
     }
-    uint4 data = win >= 0 ? w.slot_data[(size_t)win * w.npad + gi] : make_uint4(0, 0, 0, 0);
+    uint4 data = win >= 0 && scratch_ok(w, win, nslots, gi) ? w.slot_data[(size_t)win * w.npad + gi]
+                                                             : make_uint4(0, 0, 0, 0);
+    if (!BCN_GUARD(L.first + lane, L.nblocks, CHECK_BC7_STORE)) return;
     uint8_t* o = L.dst + (size_t)(L.first + lane) * 16;
     if (((uintptr_t)L.dst & 15) == 0) {
         *reinterpret_cast<uint4*>(o) = data;
@@ -458,6 +483,8 @@ __global__ void __launch_bounds__(256) bc7_select_kernel(Work w, uint32_t ntiles
 }
 
 }  // namespace bc7
+
+cudaError_t check_take_bc7(unsigned long long out[3]) { return check_record_take(out); }
 
 size_t bc7_scratch_bytes_tiles(uint32_t ntiles, const BC7SettingsDev& s) {
     const bc7::Plan P = bc7::make_plan(s);
@@ -688,11 +715,36 @@ namespace {
 static __device__ __align__(256) uint8_t g_bc7_noalloc_scratch[BC_NOALLOC_SCRATCH_BYTES];
 
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64];  // device address of the array, per device ordinal
+// Device address of the array per device ordinal, with the context it was
+// looked up in: after a device reset the device gets a new primary context,
+// the library's module is loaded again, and the address is looked up anew.
+struct NoallocAddr {
+    void* ctx;
+    void* addr;
+};
+NoallocAddr g_noalloc_addr[64];
+
+// The current context (the driver's cuCtxGetCurrent, reached through the
+// runtime, so the library needs no link against the driver library).
+typedef int (*CtxGetCurrentFn)(void**);
+void* current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (CtxGetCurrentFn)f;
+    }();
+    void* ctx = nullptr;
+    if (fn == nullptr || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 // Device address of the array on the current device. The array's name in host
 // code is only a host-side handle; the kernels need the address the runtime
-// reports for the current device, looked up once per device.
+// reports for the current device, looked up once per device (and again
+// after the device's context was replaced by a reset).
 int noalloc_scratch_address(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -701,17 +753,27 @@ int noalloc_scratch_address(void** out) {
         return BC_ERR_CUDA;
     }
     if (dev < 0 || dev >= 64) return BC_ERR_NO_DEVICE;
+    // make the device's primary context current on this thread (CUDA 12's
+    // cudaSetDevice initialises it), so the context read below is the one
+    // the launches use
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) {
+        record_cuda_error(e);
+        return BC_ERR_CUDA;
+    }
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev].addr || ctx == nullptr || g_noalloc_addr[dev].ctx != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_bc7_noalloc_scratch);
         if (e != cudaSuccess) {
             record_cuda_error(e);
             return BC_ERR_CUDA;
         }
-        g_noalloc_addr[dev] = p;
+        g_noalloc_addr[dev].addr = p;
+        g_noalloc_addr[dev].ctx = ctx;
     }
-    *out = g_noalloc_addr[dev];
+    *out = g_noalloc_addr[dev].addr;
     return BC_OK;
 }
 

@@ -11,6 +11,7 @@
 #include "bc_common.cuh"
 #include "bc_kernels.h"
 #include "bptc_decode.cuh"
+#include "bc_check.cuh"
 
 namespace bcn {
 
@@ -120,6 +121,7 @@ __global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8
 #pragma unroll
         for (int q = 0; q < kSortItems; q++) {
             uint32_t slot = s_cnt[key[q]] + wpos[q];
+            if (!BCN_GUARD(slot, G, CHECK_DECODE_SMEM)) continue;
             s_blk[slot] = v[q];
             s_orig[slot] = base + q * kSortCta + t;
         }
@@ -522,15 +524,18 @@ __global__ void __launch_bounds__(kSortCta) bc6h_decode_sorted_kernel(const uint
             continue;
         }
         uint32_t slot = cta_sort_slot(key, 18, s_cnt);
-        s_blk[slot] = v;
-        s_orig[slot] = (uint16_t)t;
+        if (BCN_GUARD(slot, kSortCta, CHECK_DECODE_SMEM)) {
+            s_blk[slot] = v;
+            s_orig[slot] = (uint16_t)t;
+        }
         __syncthreads();
         uint4 b = s_blk[t];
         uint32_t o = s_orig[t];
         uint32_t h[24];
         decode_bc6h_block<false>((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), h);
+        if (BCN_GUARD(o, kSortCta, CHECK_DECODE_SMEM))
 #pragma unroll
-        for (int q = 0; q < 24; q++) s_out[q * kSortCta + o] = h[q];
+            for (int q = 0; q < 24; q++) s_out[q * kSortCta + o] = h[q];
         __syncthreads();
         uint32_t i = base + t;
         if (i < n) {
@@ -827,4 +832,18 @@ cudaError_t launch_bc6h_error(const uint8_t* blocks, uint32_t bw, uint32_t bh, c
 
 size_t bc6h_error_partial_bytes() { return sizeof(double) * 2 * kErrCtas; }
 
+}  // namespace bcn
+
+namespace bcn {
+cudaError_t check_take_decode(unsigned long long out[3]) { return check_record_take(out); }
+
+// One guard evaluated on (index, extent) with no memory access: exercises the
+// record path of the check build (the release build records nothing).
+__global__ void check_selftest_kernel(unsigned long long index, unsigned long long extent) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) (void)BCN_GUARD(index, extent, CHECK_SELFTEST);
+}
+cudaError_t launch_check_selftest(unsigned long long index, unsigned long long extent, cudaStream_t s) {
+    check_selftest_kernel<<<1, 32, 0, s>>>(index, extent);
+    return cudaGetLastError();
+}
 }  // namespace bcn

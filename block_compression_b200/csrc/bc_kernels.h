@@ -100,6 +100,16 @@ cudaError_t launch_bc6h_error(const uint8_t* blocks, uint32_t bw, uint32_t bh, c
                               double* sums, double* block_sse, double* partial, cudaStream_t s);
 size_t bc6h_error_partial_bytes();
 
+// Check build (-DBCN_CHECK): each kernel translation unit's record of its
+// first failed bounds guard (site, index, extent), read and cleared; release
+// builds report none. launch_check_selftest evaluates one guard on the given
+// index and extent without accessing memory.
+cudaError_t check_take_bc7(unsigned long long out[3]);
+cudaError_t check_take_bc6h(unsigned long long out[3]);
+cudaError_t check_take_bc15(unsigned long long out[3]);
+cudaError_t check_take_decode(unsigned long long out[3]);
+cudaError_t launch_check_selftest(unsigned long long index, unsigned long long extent, cudaStream_t s);
+
 // Settings check shared by every BC7 entry point (BC_OK or a BC_ERR_* code),
 // and the per-thread record behind bc_last_cuda_error().
 int validate_bc7_settings(const void* settings);

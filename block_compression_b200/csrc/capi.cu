@@ -804,4 +804,34 @@ void compressor_clear(bc_compressor* c) {
 
 extern "C" int bc_last_cuda_error(void) { return t_last_cuda_error; }
 
+extern "C" int bc_check_enabled(void) {
+#ifdef BCN_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+extern "C" int bc_check_read(uint64_t out[3]) {
+    if (!out) return BC_ERR_NULL;
+    out[0] = out[1] = out[2] = 0;
+    cudaError_t (*const take[])(unsigned long long*) = {check_take_bc7, check_take_bc6h, check_take_bc15,
+                                                        check_take_decode};
+    for (auto f : take) {
+        unsigned long long r[3];
+        BC_CUDA(f(r));
+        if (r[0] != 0 && out[0] == 0) {
+            out[0] = r[0] - 1;  // site
+            out[1] = r[1];
+            out[2] = r[2];
+        }
+    }
+    return BC_OK;
+}
+
+extern "C" int bc_check_selftest(uint64_t index, uint64_t extent, void* stream) {
+    BC_CUDA(launch_check_selftest(index, extent, (cudaStream_t)stream));
+    return BC_OK;
+}
+
 extern "C" const char* bc_version(void) { return "bcn-b200 0.1.0 (sm_100a)"; }

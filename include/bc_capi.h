@@ -128,8 +128,9 @@ int bc_compress_rgba16_device(const bc_bc6h_settings* settings, const uint16_t* 
  *  - images whose scratch need exceeds BC_NOALLOC_SCRATCH_BYTES are rejected
  *    with BC_ERR_TOO_LARGE; every preset fits images up to 1024x1024 pixels;
  *  - the first call on a device looks up the array's device address (a
- *    one-time set-up per device); make that first call before any stream
- *    capture;
+ *    one-time set-up per device, repeated only when the device's context was
+ *    replaced, as after cudaDeviceReset); make that first call before any
+ *    stream capture;
  *  - all calls share the one array and it keeps the last call's contents:
  *    calls that overlap on the GPU (other streams, other host threads) race
  *    and corrupt each other's results; serialise them.
@@ -412,6 +413,20 @@ uint32_t bc_dds_dxgi_format(int variant, int srgb);
 /* ---- diagnostics -------------------------------------------------------- */
 /* cudaError_t of the last CUDA failure seen on this thread (0 if none). */
 int bc_last_cuda_error(void);
+/* Bounds-checked debug build. libbcn_b200_check.so is the same library
+ * compiled with every guarded index of the kernels (staged source rows and
+ * columns, per-block scratch rows, output blocks, decoder shared-memory
+ * slots) compared with its array's extent before the access; a failed guard
+ * records (site, index, extent) and skips the access instead of trapping.
+ * bc_check_enabled() is 1 in that build, 0 in the release build.
+ * bc_check_read() copies the first recorded failure of each kernel file
+ * since the last read into out (site, index, extent; site 0 = none) and
+ * clears the records; it synchronises. bc_check_selftest() enqueues one
+ * guard on (index, extent) that accesses no memory, to exercise the path. */
+int bc_check_enabled(void);
+int bc_check_read(uint64_t out[3]);
+int bc_check_selftest(uint64_t index, uint64_t extent, void* stream);
+
 /* Library version string, e.g. "bcn-b200 0.1.0 (sm_100a)". */
 const char* bc_version(void);
 

@@ -29,7 +29,7 @@ def test_reference_image_round_trip(bcn, oracle_lib, cuda, case):
     bcn.encode.compress_rgba8(v, img, blocks, 128, 128, 128 * 4)  # host entry point
     exp = oracle_lib.compress_rgba8(vid, img, 128, 128, settings=s)
     assert np.array_equal(blocks, exp)
-    src = torch.from_numpy(img).cuda()
+    src = torch.from_numpy(img.copy()).cuda()
     dec = torch.zeros(128 * 128 * 4, dtype=torch.uint8, device="cuda")
     bcn.decode.decompress_blocks_as_rgba8(v, 128, 128, torch.from_numpy(blocks).cuda(), dec)
     torch.cuda.synchronize()

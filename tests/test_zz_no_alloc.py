@@ -66,8 +66,16 @@ def test_noalloc_rejects_images_beyond_its_scratch(bcn, cuda):
     dst = torch.zeros((w // 4) * (h // 4) * 16, dtype=torch.uint8, device="cuda")
     assert noalloc(ctypes.byref(s), src.data_ptr(), src.numel(), dst.data_ptr(), dst.numel(), w, h, w * 4,
                    None) == -10
-    # the largest advertised size fits with the most scratch-hungry preset
+    # the largest advertised size fits with the most scratch-hungry preset,
+    # and gives the regular entry point's blocks
+    _, regular = _entry_points(bcn)
     w = h = 1024
-    assert noalloc(ctypes.byref(s), src.data_ptr(), w * h * 4, dst.data_ptr(), (w // 4) * (h // 4) * 16, w, h,
-                   w * 4, None) == 0
+    img = torch.from_numpy(synthetic.config2_image(seed=33, size=w)).cuda()
+    n = (w // 4) * (h // 4) * 16
+    want = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    got = torch.full((n,), 0xCD, dtype=torch.uint8, device="cuda")
+    assert regular(6, ctypes.cast(ctypes.byref(s), P), img.data_ptr(), img.numel(), want.data_ptr(), n, w, h, w * 4,
+                   None) == 0
+    assert noalloc(ctypes.byref(s), img.data_ptr(), img.numel(), got.data_ptr(), n, w, h, w * 4, None) == 0
     torch.cuda.synchronize()
+    assert torch.equal(got, want)
