@@ -56,10 +56,20 @@ BCN_DEV uint32_t cta_sort_slot(uint32_t key, uint32_t nkeys, uint32_t* s_cnt) {
 // blocks by mode in shared memory and decodes them in sorted order, so a
 // warp mostly runs one mode's code; each thread writes its decoded block's 4
 // texel rows (16 B each) straight to the image. Groups whose warps already
-// hold one mode each skip the sort.
-constexpr int kSortItems = 4;
+// hold one mode each keep their order (thread t decodes blocks t, t + 256,
+// ..., so the row stores of a warp are contiguous). Both cases go through
+// shared memory to a single, not unrolled decode site: the eight per-mode
+// decoders are large straight-line code, and one copy of them (instead of
+// one per unrolled item and per path) keeps the instruction cache warm.
+#ifndef BCN_BC7DEC_ITEMS
+#define BCN_BC7DEC_ITEMS 4
+#endif
+#ifndef BCN_BC7DEC_MINB
+#define BCN_BC7DEC_MINB 1
+#endif
+constexpr int kSortItems = BCN_BC7DEC_ITEMS;
 
-__global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8_t* __restrict__ blocks, uint32_t bw,
+__global__ void __launch_bounds__(kSortCta, BCN_BC7DEC_MINB) bc7_decode_sorted_kernel(const uint8_t* __restrict__ blocks, uint32_t bw,
                                                                      uint32_t bh, uint8_t* __restrict__ out,
                                                                      size_t pitch) {
     constexpr uint32_t G = kSortCta * kSortItems;
@@ -70,7 +80,7 @@ __global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8
     const uint32_t stride = gridDim.x * G;
     for (uint32_t base = blockIdx.x * G; base < n; base += stride) {
         uint4 v[kSortItems];
-        uint32_t key[kSortItems];
+        uint32_t key[kSortItems], slot[kSortItems];
         bool uniform = true;
 #pragma unroll
         for (int q = 0; q < kSortItems; q++) {
@@ -79,54 +89,43 @@ __global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8
             uint32_t low = v[q].x & 0xFFu;
             key[q] = low ? (uint32_t)__ffs((int)low) - 1u : 8u;
             uniform &= __all_sync(0xFFFFFFFFu, key[q] == __shfl_sync(0xFFFFFFFFu, key[q], 0));
+            slot[q] = q * kSortCta + t;
         }
-        if (__syncthreads_and(uniform)) {
+        if (!__syncthreads_and(uniform)) {
+            // counting sort of the G keys (warp-aggregated shared-memory atomics)
+            if (t < 32) s_cnt[t] = 0;
+            __syncthreads();
+            uint32_t wpos[kSortItems];
 #pragma unroll
             for (int q = 0; q < kSortItems; q++) {
-                uint32_t i = base + q * kSortCta + t;
-                if (i >= n) continue;
-                uint32_t px[16];
-                decode_bc7_block((uint64_t)v[q].x | ((uint64_t)v[q].y << 32), (uint64_t)v[q].z | ((uint64_t)v[q].w << 32), px);
-                uint32_t by = i / bw, bx = i - by * bw;
-#pragma unroll
-                for (int y = 0; y < 4; y++)
-                    *reinterpret_cast<uint4*>(out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16) =
-                        make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+                uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[q]);
+                uint32_t leader = __ffs((int)peers) - 1u;
+                uint32_t b = 0;
+                if (lane == leader) b = atomicAdd(&s_cnt[key[q]], (uint32_t)__popc(peers));
+                wpos[q] = __shfl_sync(0xFFFFFFFFu, b, (int)leader) + __popc(peers & ((1u << lane) - 1u));
             }
-            continue;
+            __syncthreads();
+            if (t < 32) {
+                uint32_t c = t < 9 ? s_cnt[t] : 0u, x = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                    if (lane >= (uint32_t)o) x += y;
+                }
+                s_cnt[t] = x - c;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < kSortItems; q++) slot[q] = s_cnt[key[q]] + wpos[q];
         }
-        // counting sort of the G keys (warp-aggregated shared-memory atomics)
-        if (t < 32) s_cnt[t] = 0;
-        __syncthreads();
-        uint32_t wpos[kSortItems];
 #pragma unroll
         for (int q = 0; q < kSortItems; q++) {
-            uint32_t peers = __match_any_sync(0xFFFFFFFFu, key[q]);
-            uint32_t leader = __ffs((int)peers) - 1u;
-            uint32_t b = 0;
-            if (lane == leader) b = atomicAdd(&s_cnt[key[q]], (uint32_t)__popc(peers));
-            wpos[q] = __shfl_sync(0xFFFFFFFFu, b, (int)leader) + __popc(peers & ((1u << lane) - 1u));
+            if (!BCN_GUARD(slot[q], G, CHECK_DECODE_SMEM)) continue;
+            s_blk[slot[q]] = v[q];
+            s_orig[slot[q]] = base + q * kSortCta + t;
         }
         __syncthreads();
-        if (t < 32) {
-            uint32_t c = t < 9 ? s_cnt[t] : 0u, x = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if (lane >= (uint32_t)o) x += y;
-            }
-            s_cnt[t] = x - c;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < kSortItems; q++) {
-            uint32_t slot = s_cnt[key[q]] + wpos[q];
-            if (!BCN_GUARD(slot, G, CHECK_DECODE_SMEM)) continue;
-            s_blk[slot] = v[q];
-            s_orig[slot] = base + q * kSortCta + t;
-        }
-        __syncthreads();
-#pragma unroll
+#pragma unroll 1
         for (int q = 0; q < kSortItems; q++) {
             uint4 b = s_blk[q * kSortCta + t];
             uint32_t i = s_orig[q * kSortCta + t];
@@ -134,6 +133,7 @@ __global__ void __launch_bounds__(kSortCta) bc7_decode_sorted_kernel(const uint8
                 uint32_t px[16];
                 decode_bc7_block((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), px);
                 uint32_t by = i / bw, bx = i - by * bw;
+                if (!BCN_GUARD(by, bh, CHECK_DECODE_STORE)) continue;
 #pragma unroll
                 for (int y = 0; y < 4; y++)
                     *reinterpret_cast<uint4*>(out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16) =
