@@ -18,18 +18,31 @@ using namespace bptc;
 // the alpha row, chosen once per candidate. Volatile reads: every use is a
 // shared-memory load, so the compiler keeps no register copy of the block
 // across the refinement loops (which cost this long kernel spills).
+// The packed pixel words get the same rotation with one byte permute (byte c
+// <- byte 3 for c = rot; byte 3 is outside the 3 channels read), and the
+// channel square sums are read from the rotated channel's row.
 template <bool CH4>
 struct BlkRot {
     const float* p;
     int o[3];
+    uint32_t sel;
     BCN_DEV BlkRot(const float* pxlane, int rot) : p(pxlane) {
+        sel = 0x3210u;
 #pragma unroll
-        for (int c = 0; c < 3; c++) o[c] = (c == rot ? 48 : c * 16) * NB;
+        for (int c = 0; c < 3; c++) {
+            o[c] = (c == rot ? 48 : c * 16) * NB;
+            if (c == rot) sel = (sel & ~(0xFu << (4 * c))) | (3u << (4 * c));
+        }
     }
     BCN_DEV float operator()(int c, int k) const {
         const volatile float* q = p + o[c];
         return q[k * NB];
     }
+    BCN_DEV uint32_t packed(int k) const {
+        const volatile float* q = p + PX_PACKED * NB;
+        return __byte_perm(__float_as_uint(q[k * NB]), 0u, sel);
+    }
+    BCN_DEV int sq(int c) const { return __float_as_int(p[PX_SQ * NB + (o[c] >> 4)]); }
 };
 
 // ---- endpoint quantisation (bc7.rs:97-237) ----------------------------------

@@ -49,7 +49,7 @@
 #ifndef BCN_REFINE_WARPS  // warps (tiles) per CTA of the refine and mode-6 kernels
 #define BCN_REFINE_WARPS 4
 #endif
-static_assert(BCN_REFINE_WARPS >= 1 && BCN_REFINE_WARPS <= 5, "8 KiB of static shared memory per warp, 48 KiB at most");
+static_assert(BCN_REFINE_WARPS >= 1 && BCN_REFINE_WARPS <= 4, "10.5 KiB of static shared memory per warp, 48 KiB at most");
 #ifndef BCN_MODE6_MINB
 #define BCN_MODE6_MINB 4
 #endif
@@ -171,7 +171,9 @@ BCN_DEV int nslots_of(const Plan& P) { return 5 + P.n45_4 + P.n45_5 + 1; }
 
 // Stages the 32 blocks of `tile` into px (planar f32, lane-strided) with
 // threads tid = 0..nt-1 (128-bit loads: the 4 rows of 32 neighbouring blocks
-// are 4 contiguous 512-byte spans).
+// are 4 contiguous 512-byte spans). PK: also rows PX_PACKED.. (the pixel
+// words as loaded), for the integer index fit.
+template <bool PK = true>
 BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, int nt) {
     const TileLoc L = tile_loc(w, tile);
     for (int t = tid; t < NB * 4; t += nt) {
@@ -202,7 +204,21 @@ BCN_DEV void stage_tile(float (*px)[NB], const Work& w, uint32_t tile, int tid, 
             px[16 + k][b] = (float)((v[x] >> 8) & 0xFF);
             px[32 + k][b] = (float)((v[x] >> 16) & 0xFF);
             px[48 + k][b] = (float)(v[x] >> 24);
+            if (PK) px[PX_PACKED + k][b] = __uint_as_float(v[x]);
         }
+    }
+}
+
+// Rows PX_SQ..PX_SQ+3 of a staged tile: per block and channel, the sum of
+// the squares of its 16 values (exact integers, below 2^24), stored as int
+// bits. Threads tid = 0..nt-1, after the staged rows are visible to them.
+BCN_DEV void stage_channel_squares(float (*px)[NB], int tid, int nt) {
+    for (int t = tid; t < 4 * NB; t += nt) {
+        const int c = t >> 5, b = t & 31;
+        float s = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) s = fmaf(px[c * 16 + k][b], px[c * 16 + k][b], s);
+        px[PX_SQ + c][b] = __int_as_float((int)s);
     }
 }
 
@@ -224,7 +240,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
-    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    stage_tile<false>(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
     const Blk blk{&px[0][lane]};
     if (P.bounds_a && P.bounds_b) {
@@ -310,7 +326,7 @@ __global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_S
     bc7_search_kernel(Work w) {
     constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
     constexpr bool two = ModeTraits<MODE>::pairs == 2;
-    __shared__ float px[64][NB];
+    __shared__ float px[PX_ROWS][NB];
     __shared__ float full[two ? 15 : 1][NB];
     __shared__ unsigned long long best[NW][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -319,11 +335,12 @@ __global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_S
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
     const Blk blk{&px[0][lane]};
-    if (two) {
-        // the whole block's statistics, one entry per warp at a time
+    // the whole block's statistics (two subsets), one entry per warp at a
+    // time, and the channel square sums
+    if (two)
         for (int e = warp; e < 15; e += NW) full[e][lane] = stat_entry<ModeTraits<MODE>::ch>(blk, e);
-        __syncthreads();
-    }
+    stage_channel_squares(px, threadIdx.x, NW * 32);
+    __syncthreads();
     const int c = blockIdx.y * NW + warp;
     unsigned long long key = ~0ull;
     if (c < P.count[mi] && tile_loc(w, tile).valid(lane)) {
@@ -348,11 +365,13 @@ __global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_S
 template <int MODE, int NW>
 __global__ void __launch_bounds__(NW * 32, BCN_REFINE_MINB) bc7_refine_kernel(Work w, uint32_t ntiles) {
     constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
-    __shared__ float px[NW][64][NB];
+    __shared__ float px[NW][PX_ROWS][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x * NW + warp;
     if (tile >= ntiles) return;
     stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    stage_channel_squares(px[warp], lane, 32);
     __syncwarp();
     const uint32_t gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
@@ -378,7 +397,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_REFINE_MINB) bc7_refine_kernel(Wo
 // rotation for the tile's 32 blocks.
 template <int MODE, int SWAP, bool CH4, int NW>
 __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Work w) {
-    __shared__ float px[64][NB];
+    __shared__ float px[PX_ROWS][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
@@ -386,8 +405,14 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Wo
     if (!CH4) {
         // 3-channel settings: the rotated-out channel reads 255 (BlkRot)
         __syncthreads();
-        for (int t = threadIdx.x; t < 16 * NB; t += NW * 32) px[48 + t / NB][t % NB] = 255.0f;
+        for (int t = threadIdx.x; t < 16 * NB; t += NW * 32) {
+            px[48 + t / NB][t % NB] = 255.0f;
+            px[PX_PACKED + t / NB][t % NB] =
+                __uint_as_float(__float_as_uint(px[PX_PACKED + t / NB][t % NB]) | 0xFF000000u);
+        }
     }
+    __syncthreads();
+    stage_channel_squares(px, threadIdx.x, NW * 32);
     __syncthreads();
     const int r = blockIdx.y * NW + warp;  // rotation index
     if (r >= P.n45_5) return;              // n45_5 = number of rotations
@@ -407,11 +432,13 @@ __global__ void __launch_bounds__(NW * 32, BCN_MODE45_MINB) bc7_mode45_kernel(Wo
 // K5: mode 6 (bc7.rs:762-817), one warp per tile.
 template <int CH, int NW>
 __global__ void __launch_bounds__(NW * 32, BCN_MODE6_MINB) bc7_mode6_kernel(Work w, uint32_t ntiles) {
-    __shared__ float px[NW][64][NB];
+    __shared__ float px[NW][PX_ROWS][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x * NW + warp;
     if (tile >= ntiles) return;
     stage_tile(px[warp], w, tile, lane, 32);
+    __syncwarp();
+    stage_channel_squares(px[warp], lane, 32);
     __syncwarp();
     const Plan P = make_plan(w.S);
     const uint32_t gi = tile * NB + lane;

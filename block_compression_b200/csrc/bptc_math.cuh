@@ -10,10 +10,16 @@ namespace bptc {
 
 constexpr int NB = 32;  // blocks per tile; lane l of each warp owns block l
 
-// Planar view of one block in shared memory: channel c, pixel k.
+// Planar view of one block in shared memory: channel c, pixel k. The BC7
+// kernels also stage rows PX_PACKED.. (each pixel's four bytes in one word)
+// and PX_SQ.. (per channel, the sum of the squares of its 16 values), which
+// the integer index fit reads through packed() and sq().
+constexpr int PX_PACKED = 64, PX_SQ = 80, PX_ROWS = 84;
 struct Blk {
     const float* p;
     BCN_DEV float operator()(int c, int k) const { return p[(c * 16 + k) * NB]; }
+    BCN_DEV uint32_t packed(int k) const { return __float_as_uint(p[(PX_PACKED + k) * NB]); }
+    BCN_DEV int sq(int c) const { return __float_as_int(p[(PX_SQ + c) * NB]); }
 };
 
 // ---- shared math (src/encode/common.rs) -------------------------------------
@@ -283,44 +289,117 @@ BCN_DEV void pixel_err2(int bs, int df, float v, int w0, int w1, int& err0, int&
     err1 += a1 * a1;
 }
 
-// One pixel of block_quant's integer path (pixels and endpoints bytes):
-// vi the pixel's channels, ia / df the pair's low endpoint and
-// high - low endpoint per channel, dv / rdv the pair's squared length and
-// its reciprocal. With t = v - ia every projection term t * df is an exact
-// integer and so is their sum (at most 4 * 255^2): the float sum the
-// reference forms is that integer. The quotient by dv is the reciprocal and
-// one fused correction step (exact for all such integer pairs), and the
-// decoded-value errors are pixel_err2's with bs - 64 * v = 32 - 64 * t.
-// Returns the chosen index; be = its squared error.
-template <int CH, int BITS>
-BCN_DEV int fit_pixel_int(const int* vi, const int* ia, const int* df, float dv, float rdv, int& be) {
+// Index-fit constants of one endpoint pair for 8-bit pixels and endpoints
+// (ia / ib the pair's two endpoints per channel, df = ib - ia; channels at
+// and above CH are 0 throughout):
+//   pos, neg    max(df, 0) and max(-df, 0) per channel, one byte each;
+//   nbase       -sum ia * df;
+//   dv, rdv     sum df^2 in the reference's operation order, RN(1 / dv);
+//   bs01, bs23  4 * (64 * ia + 32) of channels 0/1 (2/3) in the low / high
+//               16-bit half;
+//   df01, df23  the integer 4 * df_0 + 2^16 * 4 * df_1 (2/3) mod 2^32.
+struct FitPair {
+    uint32_t pos, neg, bs01, bs23, df01, df23;
+    int nbase;
+    float dv, rdv;
+};
+
+template <int CH>
+BCN_DEV FitPair fit_pair(const float* ep) {
+    FitPair f;
+    int ia[4] = {0, 0, 0, 0}, df[4] = {0, 0, 0, 0};
+    float div = 0.0f;
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        const float d = ep[4 + p] - ep[p];
+        div += sqf(d);
+        ia[p] = (int)ep[p];
+        df[p] = (int)ep[4 + p] - ia[p];
+    }
+    f.dv = div;
+    f.rdv = __frcp_rn(div);
+    f.pos = 0;
+    f.neg = 0;
+    f.nbase = 0;
+#pragma unroll
+    for (int p = 0; p < CH; p++) {
+        f.pos |= (uint32_t)max(df[p], 0) << (8 * p);
+        f.neg |= (uint32_t)max(-df[p], 0) << (8 * p);
+        f.nbase -= ia[p] * df[p];
+    }
+    uint32_t bs[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) bs[p] = p < CH ? (uint32_t)(256 * ia[p] + 128) : 0u;
+    f.bs01 = bs[0] + (bs[1] << 16);
+    f.bs23 = bs[2] + (bs[3] << 16);
+    f.df01 = (uint32_t)(4 * df[0]) + ((uint32_t)(4 * df[1]) << 16);
+    f.df23 = (uint32_t)(4 * df[2]) + ((uint32_t)(4 * df[3]) << 16);
+    return f;
+}
+
+template <int PAIRS>
+BCN_DEV FitPair sel_fit(int j, const FitPair* f) {
+    const FitPair& a = f[0];
+    const FitPair& b = f[PAIRS > 1 ? 1 : 0];
+    const FitPair& c = f[PAIRS > 2 ? 2 : 0];
+    FitPair r;
+    r.pos = sel_pair<PAIRS>(j, a.pos, b.pos, c.pos);
+    r.neg = sel_pair<PAIRS>(j, a.neg, b.neg, c.neg);
+    r.bs01 = sel_pair<PAIRS>(j, a.bs01, b.bs01, c.bs01);
+    r.bs23 = sel_pair<PAIRS>(j, a.bs23, b.bs23, c.bs23);
+    r.df01 = sel_pair<PAIRS>(j, a.df01, b.df01, c.df01);
+    r.df23 = sel_pair<PAIRS>(j, a.df23, b.df23, c.df23);
+    r.nbase = sel_pair<PAIRS>(j, a.nbase, b.nbase, c.nbase);
+    r.dv = sel_pair<PAIRS>(j, a.dv, b.dv, c.dv);
+    r.rdv = sel_pair<PAIRS>(j, a.rdv, b.rdv, c.rdv);
+    return r;
+}
+
+// One pixel of block_quant's integer path: v = the pixel's bytes packed in a
+// word (channels at and above the pair's CH are ignored: their pos, neg, bs
+// and df bytes are 0). Every quantity is an exact integer:
+//   * the projection sum (v - ia) . df is sum v * df - sum ia * df, with
+//     sum v * df = v . pos - v . neg (byte dot products); the reference's
+//     float sum of exact integer terms is that integer. The quotient by dv is
+//     the reciprocal and one fused correction step (exact for all such
+//     integer pairs);
+//   * the decoded value of index weight w is d = (64 * ia + 32 + w * df) >> 6,
+//     and 4 * (64 * ia + 32 + w * df) lies in [128, 65408], so
+//     bs01 + w * df01 holds it for channels 0 and 1 in its two 16-bit halves
+//     (no borrow between them) and byte 1 of each half is d: one byte permute
+//     gathers the four decoded channels d (0 above CH);
+//   * the squared error sum (d - v)^2 over the channels is
+//     d . d - 2 d . v + v . v; the last term is the same for both candidate
+//     indices and is added once per block by the caller.
+// So the index chosen and its error are the reference's (errors compared
+// with the same strict "<"). Returns the index; be = its error minus v . v.
+template <int BITS>
+BCN_DEV uint32_t fit_pixel_pk(uint32_t v, const FitPair& f, int& be) {
     constexpr int levels = 1 << BITS;
-    int t[CH], pi = 0;
-#pragma unroll
-    for (int p = 0; p < CH; p++) {
-        t[p] = vi[p] - ia[p];
-        pi += t[p] * df[p];
-    }
-    float proj = (float)pi;
-    const float q = proj * rdv;
-    proj = fmaf(fmaf(-q, dv, proj), rdv, q);
+    float proj = (float)(int)(__dp4a(v, f.pos, (uint32_t)f.nbase) - __dp4a(v, f.neg, 0u));
+    const float q = proj * f.rdv;
+    proj = fmaf(fmaf(-q, f.dv, proj), f.rdv, q);
     const int q1i = clampi((int)(proj * (float)levels + 0.5f), 1, levels - 1);
-    const int w0 = bptc_w<BITS>(q1i - 1), w1 = bptc_w<BITS>(q1i);
-    int err0 = 0, err1 = 0;
-#pragma unroll
-    for (int p = 0; p < CH; p++) {
-        const int bsv = 32 - 64 * t[p];
-        const int a0 = (bsv + w0 * df[p]) >> 6, a1 = (bsv + w1 * df[p]) >> 6;
-        err0 += a0 * a0;
-        err1 += a1 * a1;
-    }
-    be = err1;
-    int bq = q1i;
-    if (err0 < err1) {
-        be = err0;
-        bq = q1i - 1;
+    const uint32_t w0 = (uint32_t)bptc_w<BITS>(q1i - 1), w1 = (uint32_t)bptc_w<BITS>(q1i);
+    const uint32_t d0 = __byte_perm(f.bs01 + w0 * f.df01, f.bs23 + w0 * f.df23, 0x7531);
+    const uint32_t d1 = __byte_perm(f.bs01 + w1 * f.df01, f.bs23 + w1 * f.df23, 0x7531);
+    const int e0 = (int)__dp4a(d0, d0, 0u) - 2 * (int)__dp4a(d0, v, 0u);
+    const int e1 = (int)__dp4a(d1, d1, 0u) - 2 * (int)__dp4a(d1, v, 0u);
+    be = e1;
+    uint32_t bq = (uint32_t)q1i;
+    if (e0 < e1) {
+        be = e0;
+        bq = (uint32_t)q1i - 1u;
     }
     return bq;
+}
+
+// sum over the block's pixels of v . v over the first CH channels
+template <int CH, class B>
+BCN_DEV int block_sq(const B& blk) {
+    int s = blk.sq(0) + blk.sq(1) + blk.sq(2);
+    if (CH == 4) s += blk.sq(3);
+    return s;
 }
 
 // common.rs:422-481. ep holds PAIRS endpoint pairs at stride 8, dequantised
@@ -330,53 +409,32 @@ BCN_DEV int fit_pixel_int(const int* vi, const int* ia, const int* df, float dv,
 // interpolation (64 - w) * ia + w * ib + 32 written as
 // (64 * ia + 32) + w * (ib - ia), which is non-negative, so / 64 is >> 6.
 // INT: pixels and endpoints are 8-bit integers (BC7), so each pixel is
-// fitted in integer arithmetic by fit_pixel_int (the projection is an
-// integer divided by an integer, both at most 4 * 255^2 in magnitude, taken
-// with the divisor's reciprocal and one fused correction step, which equals
-// the IEEE quotient over that whole domain -- checked exhaustively by the
-// oracle test -- and the pixel errors and their total are exact integers).
-// Otherwise the float path with IEEE division (BC6H).
+// fitted in integer arithmetic by fit_pixel_pk from the block's packed
+// pixel words (the projection is an integer divided by an integer, both at
+// most 4 * 255^2 in magnitude, taken with the divisor's reciprocal and one
+// fused correction step, which equals the IEEE quotient over that whole
+// domain -- checked exhaustively by the oracle test -- and the pixel errors
+// and their total are exact integers, below 2^24). Otherwise the float path
+// with IEEE division (BC6H).
 template <int CH, int BITS, int PAIRS, bool INT = false, class B>
 BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
-    if (INT) {
-        int ia[PAIRS][CH], df[PAIRS][CH];
-        float dv[PAIRS], rdv[PAIRS];
+    if constexpr (INT) {
+        FitPair fp[PAIRS];
 #pragma unroll
-        for (int j = 0; j < PAIRS; j++) {
-            float div = 0.0f;
-#pragma unroll
-            for (int p = 0; p < CH; p++) {
-                const float d = ep[8 * j + 4 + p] - ep[8 * j + p];
-                div += sqf(d);
-                ia[j][p] = (int)ep[8 * j + p];
-                df[j][p] = (int)ep[8 * j + 4 + p] - ia[j][p];
-            }
-            dv[j] = div;
-            rdv[j] = __frcp_rn(div);
-        }
+        for (int j = 0; j < PAIRS; j++) fp[j] = fit_pair<CH>(ep + 8 * j);
         int total = 0;
         q0 = 0;
         q1 = 0;
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             const int j = PAIRS == 1 ? 0 : (int)((pattern >> (2 * k)) & 3);
-            int vi[CH], a[CH], f[CH];
-#pragma unroll
-            for (int p = 0; p < CH; p++) {
-                // indices stay inside the PAIRS rows
-                vi[p] = (int)blk(p, k);
-                a[p] = sel_pair<PAIRS>(j, ia[0][p], ia[PAIRS > 1 ? 1 : 0][p], ia[PAIRS > 2 ? 2 : 0][p]);
-                f[p] = sel_pair<PAIRS>(j, df[0][p], df[PAIRS > 1 ? 1 : 0][p], df[PAIRS > 2 ? 2 : 0][p]);
-            }
             int be;
-            const uint32_t bq = (uint32_t)fit_pixel_int<CH, BITS>(
-                vi, a, f, sel_pair<PAIRS>(j, dv[0], dv[PAIRS > 1 ? 1 : 0], dv[PAIRS > 2 ? 2 : 0]),
-                sel_pair<PAIRS>(j, rdv[0], rdv[PAIRS > 1 ? 1 : 0], rdv[PAIRS > 2 ? 2 : 0]), be);
+            const uint32_t bq = fit_pixel_pk<BITS>(blk.packed(k), sel_fit<PAIRS>(j, fp), be);
             if (k < 8) q0 |= bq << (4 * k);
             else q1 |= bq << (4 * (k - 8));
             total += be;
         }
-        return (float)total;
+        return (float)(total + block_sq<CH>(blk));
     }
     // float path (BC6H): IEEE division
     constexpr int levels = 1 << BITS;
@@ -449,30 +507,18 @@ BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t patt
     q1 = 0;
 #pragma unroll
     for (int j = 0; j < PAIRS; j++) {
-        int ia[CH], df[CH];
-        float div = 0.0f;
-#pragma unroll
-        for (int p = 0; p < CH; p++) {
-            const float d = ep[8 * j + 4 + p] - ep[8 * j + p];
-            div += sqf(d);
-            ia[p] = (int)ep[8 * j + p];
-            df[p] = (int)ep[8 * j + 4 + p] - ia[p];
-        }
-        const float rdv = __frcp_rn(div);
+        const FitPair f = fit_pair<CH>(ep + 8 * j);
         const uint32_t mask = PAIRS == 1 ? 0xFFFFu : subset_mask_from_map(pattern, j);
         for (uint32_t m = mask; m; m &= m - 1) {
             const int k = __ffs(m) - 1;
-            int vi[CH];
-#pragma unroll
-            for (int p = 0; p < CH; p++) vi[p] = (int)blk(p, k);
             int be;
-            const uint32_t bq = (uint32_t)fit_pixel_int<CH, BITS>(vi, ia, df, div, rdv, be);
+            const uint32_t bq = fit_pixel_pk<BITS>(blk.packed(k), f, be);
             if (k < 8) q0 |= bq << (4 * k);
             else q1 |= bq << (4 * (k - 8));
             total += be;
         }
     }
-    return (float)total;
+    return (float)(total + block_sq<CH>(blk));
 }
 
 // common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH). INT: 8-bit pixels
