@@ -26,12 +26,13 @@ struct BlkRot {
     const float* p;
     int o[3];
     uint32_t sel;
-    BCN_DEV BlkRot(const float* pxlane, int rot) : p(pxlane) {
+    int rot;
+    BCN_DEV BlkRot(const float* pxlane, int rot_) : p(pxlane), rot(rot_) {
         sel = 0x3210u;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            o[c] = (c == rot ? 48 : c * 16) * NB;
-            if (c == rot) sel = (sel & ~(0xFu << (4 * c))) | (3u << (4 * c));
+            o[c] = (c == rot_ ? 48 : c * 16) * NB;
+            if (c == rot_) sel = (sel & ~(0xFu << (4 * c))) | (3u << (4 * c));
         }
     }
     BCN_DEV float operator()(int c, int k) const {
@@ -43,6 +44,16 @@ struct BlkRot {
         return __byte_perm(__float_as_uint(q[k * NB]), 0u, sel);
     }
     BCN_DEV int sq(int c) const { return __float_as_int(p[PX_SQ * NB + (o[c] >> 4)]); }
+    // channels 0-2 of pixels 4g..4g+3 after the rotation, one byte per pixel
+    BCN_DEV void group_bytes(int g, uint32_t c[4]) const {
+        const volatile float* q = p + PX_PACKED * NB;
+        uint32_t o4[4];
+        transpose_bytes4(__float_as_uint(q[(4 * g) * NB]), __float_as_uint(q[(4 * g + 1) * NB]),
+                         __float_as_uint(q[(4 * g + 2) * NB]), __float_as_uint(q[(4 * g + 3) * NB]), o4);
+#pragma unroll
+        for (int ch = 0; ch < 3; ch++) c[ch] = ch == rot ? o4[3] : o4[ch];
+        c[3] = o4[3];
+    }
 };
 
 // ---- endpoint quantisation (bc7.rs:97-237) ----------------------------------
@@ -111,33 +122,36 @@ BCN_DEV void quant245(int* qep, const float* ep) {
     for (int i = 0; i < N; i++) qep[i] = clampi((int)(div_const<255>(ep[i]) * (float)(levels - 1) + 0.5f), 0, levels - 1);
 }
 
-// ep_quant_dequant for the partitioned modes over PAIRS pairs; channel 3 is
-// handled only for mode 7 (4 channels).
+// ep_quant_dequant (bc7.rs:102-237) of one endpoint pair of a partitioned
+// mode: q = the quantised endpoints, e = their dequantised values; channel 3
+// is handled only for mode 7 (4 channels).
+template <int MODE>
+BCN_DEV void quant_dequant_pair(int* q, float* e) {
+    if (MODE == 0) quant0367_pair<4, 3, 3, true>(q, e);
+    else if (MODE == 3) quant0367_pair<7, 3, 3, false>(q, e);
+    else if (MODE == 7) quant0367_pair<5, 4, 4, false>(q, e);
+    else if (MODE == 1) quant1_pair(q, e);
+    else {
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if ((i & 3) != 3) q[i] = clampi((int)(div_const<255>(e[i]) * 31.0f + 0.5f), 0, 31);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        if (MODE != 7 && (i & 3) == 3) continue;
+        if (MODE == 3) e[i] = (float)q[i];
+        else if (MODE == 1) e[i] = (float)unpack_to_byte(q[i], 7);
+        else if (MODE == 7) e[i] = (float)unpack_to_byte(q[i], 6);
+        else e[i] = (float)unpack_to_byte(q[i], 5);
+    }
+}
+
+// ep_quant_dequant for the partitioned modes over all their pairs.
 template <int MODE>
 BCN_DEV void quant_dequant_part(int qep[24], float ep[24]) {
     constexpr int pairs = (MODE == 0 || MODE == 2) ? 3 : 2;
 #pragma unroll
-    for (int j = 0; j < pairs; j++) {
-        int* q = qep + 8 * j;
-        float* e = ep + 8 * j;
-        if (MODE == 0) quant0367_pair<4, 3, 3, true>(q, e);
-        else if (MODE == 3) quant0367_pair<7, 3, 3, false>(q, e);
-        else if (MODE == 7) quant0367_pair<5, 4, 4, false>(q, e);
-        else if (MODE == 1) quant1_pair(q, e);
-        else {
-#pragma unroll
-            for (int i = 0; i < 8; i++)
-                if ((i & 3) != 3) q[i] = clampi((int)(div_const<255>(e[i]) * 31.0f + 0.5f), 0, 31);
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            if (MODE != 7 && (i & 3) == 3) continue;
-            if (MODE == 3) e[i] = (float)q[i];
-            else if (MODE == 1) e[i] = (float)unpack_to_byte(q[i], 7);
-            else if (MODE == 7) e[i] = (float)unpack_to_byte(q[i], 6);
-            else e[i] = (float)unpack_to_byte(q[i], 5);
-        }
-    }
+    for (int j = 0; j < pairs; j++) quant_dequant_pair<MODE>(qep + 8 * j, ep + 8 * j);
 }
 
 // ---- candidate evaluation of modes 0/1/2/3/7 (bc7.rs:517-538) -----------------
@@ -149,41 +163,67 @@ struct ModeTraits {
     static constexpr int ch = MODE == 7 ? 4 : 3;
 };
 
-// UNIFORM: every lane of the warp evaluates the same partition.
-template <int MODE, bool UNIFORM = false, class B>
-BCN_DEV float eval_part(const B& blk, const uint32_t* map, int part_id, int qep[24], uint32_t& q0, uint32_t& q1,
-                        const float* full = nullptr) {
+// Unquantised endpoints (block_segment of each subset, bc7.rs:517-538) of a
+// two-subset partition (modes 1, 3, 7) into ep[0..7] and ep[8..15], given
+// the whole block's statistics (full[i * NB], lane-strided like the pixels).
+// Every statistic is a sum of 8-bit values or of their products, an integer
+// below 2^24 however it is summed, so the larger subset's statistics are the
+// whole block's minus the smaller one's, bit for bit. Only the smaller
+// subset is summed, which also bounds the warp's divergent loop (each lane
+// has its own partition here) by 8 pixels. The result depends on the
+// channel count only, not on the mode: modes 1 and 3 share it.
+template <int CH, class B>
+BCN_DEV void segment_part2(const B& blk, uint32_t pattern, const float* full, float ep[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) ep[i] = 0.0f;
+    const uint32_t m1 = subset_mask_from_map(pattern, 1), m0 = ~m1 & 0xFFFFu;
+    const bool small1 = __popc(m1) <= 8;
+    float ss[15], st[15];
+    stats_masked<CH, true>(blk, small1 ? m1 : m0, ss);
+#pragma unroll
+    for (int i = 0; i < 15; i++) st[i] = small1 ? full[i * NB] - ss[i] : ss[i];
+    block_segment_from_stats<CH, true, true>(blk, m0, st, ep);
+#pragma unroll
+    for (int i = 0; i < 15; i++) st[i] = small1 ? ss[i] : full[i * NB] - ss[i];
+    block_segment_from_stats<CH, true, true>(blk, m1, st, ep + 8);
+}
+
+// Quantisation and index fit of a two-subset candidate from its unquantised
+// endpoints (ep is overwritten with the dequantised ones): its error.
+template <int MODE, class B>
+BCN_DEV float quant_fit_part2(const B& blk, uint32_t pattern, float ep[16]) {
     using T = ModeTraits<MODE>;
-    float ep[24];
+    static_assert(T::pairs == 2, "two-subset modes");
+    int qep[16];
 #pragma unroll
-    for (int i = 0; i < 24; i++) ep[i] = 0.0f;
-    uint32_t pattern = map[part_id];
-    if (T::pairs == 2 && full != nullptr) {
-        // Two subsets, the whole block's statistics given (full[i * NB],
-        // lane-strided like the pixels). Every statistic is a sum of 8-bit
-        // values or of their products, an integer below 2^24 however it is
-        // summed, so the larger subset's statistics are the whole block's
-        // minus the smaller one's, bit for bit. Only the smaller subset is
-        // summed, which also bounds the warp's divergent loop (each lane has
-        // its own partition here) by 8 pixels.
-        const uint32_t m1 = subset_mask_from_map(pattern, 1), m0 = ~m1 & 0xFFFFu;
-        const bool small1 = __popc(m1) <= 8;
-        float ss[15], st[15];
-        stats_masked<T::ch, true>(blk, small1 ? m1 : m0, ss);
-#pragma unroll
-        for (int i = 0; i < 15; i++) st[i] = small1 ? full[i * NB] - ss[i] : ss[i];
-        block_segment_from_stats<T::ch, true, true>(blk, m0, st, ep);
-#pragma unroll
-        for (int i = 0; i < 15; i++) st[i] = small1 ? ss[i] : full[i * NB] - ss[i];
-        block_segment_from_stats<T::ch, true, true>(blk, m1, st, ep + 8);
-    } else {
-#pragma unroll
-        for (int j = 0; j < T::pairs; j++)
-            block_segment<T::ch, true, true>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
+    for (int j = 0; j < 2; j++) quant_dequant_pair<MODE>(qep + 8 * j, ep + 8 * j);
+    uint32_t q0, q1;
+    return block_quant<T::ch, T::bits, 2, true>(blk, ep, pattern, q0, q1);
+}
+
+// One subset (pixel mask) of a mode-0 / mode-2 candidate: its endpoint fit
+// (block_segment), quantisation and index fit, as the reference does them
+// for each subset of a partition. Everything here depends only on the
+// subset's pixels, so a subset shared by several partitions gives them the
+// same result. Returns the subset's index-fit error minus its pixels' v . v
+// (an exact integer; the partition's error is the sum over its subsets plus
+// the block's v . v).
+template <int MODE, class B>
+BCN_DEV int eval_subset(const B& blk, uint32_t mask) {
+    static_assert(MODE == 0 || MODE == 2, "three-subset modes");
+    using T = ModeTraits<MODE>;
+    float ep[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    block_segment<T::ch, true, true>(blk, mask, ep);
+    int qep[8];
+    quant_dequant_pair<MODE>(qep, ep);
+    const FitPair f = fit_pair<T::ch>(ep);
+    int total = 0;
+    for (uint32_t m = mask; m; m &= m - 1) {
+        int be;
+        fit_pixel_pk<T::bits>(blk.packed(__ffs(m) - 1), f, be);
+        total += be;
     }
-    quant_dequant_part<MODE>(qep, ep);
-    if (UNIFORM) return block_quant_by_subset<T::ch, T::bits, T::pairs>(blk, ep, pattern, q0, q1);
-    return block_quant<T::ch, T::bits, T::pairs, true>(blk, ep, pattern, q0, q1);
+    return total;
 }
 
 // bc7.rs:381-440

@@ -10,10 +10,13 @@
 //
 //   prep     PCA split bounds of the 64 partitions, ascending top-k lists
 //            (modes 1/3/7)
-//   search   one launch per mode 0/2/1/3/7; grid (tile, candidate group), a
-//            warp evaluates one partition candidate for 32 blocks; the first
-//            minimum per block is kept with a 64-bit atomicMin on
-//            (error bits << 32 | candidate)
+//   search   modes 1/3/7 (modes 1 and 3 in one launch); grid (tile,
+//            candidate group), a warp evaluates one partition candidate for
+//            32 blocks; the first minimum per block is kept with a 64-bit
+//            atomicMin on (error bits << 32 | candidate). Modes 0/2 (three
+//            subsets, fixed partition order): one CTA per tile evaluates
+//            each distinct subset of the searched partitions once and sums
+//            them per partition
 //   refine   one launch per mode: refinement of each block's winner + coding
 //   mode4/5  rotation / index-swap candidates, one warp per candidate
 //   mode6    one warp per tile
@@ -61,6 +64,12 @@ static_assert(BCN_REFINE_WARPS >= 1 && BCN_REFINE_WARPS <= 4, "10.5 KiB of stati
 #endif
 #ifndef BCN_SEARCH7_MINB  // mode 7 (4 channels) needs more registers
 #define BCN_SEARCH7_MINB 5
+#endif
+#ifndef BCN_SEARCH3_WARPS  // warps per CTA of the mode 0/2 search (36 and 140 distinct subsets)
+#define BCN_SEARCH3_WARPS 12
+#endif
+#ifndef BCN_SEARCH3_MINB
+#define BCN_SEARCH3_MINB 4
 #endif
 namespace bcn {
 namespace bc7 {
@@ -315,49 +324,145 @@ BCN_DEV int part_of(const Work& w, int mi, int c, uint32_t gi, const Plan& P) {
     return scratch_ok(w, row, P.k_a + P.k_b, gi) ? w.lists[(size_t)row * w.npad + gi] : 0;
 }
 
-// K2: every partition candidate of one mode (bc7.rs:517-569). Grid: (tile,
-// candidate group); warp w evaluates candidate blockIdx.y*NW+w for the 32
-// blocks of the tile. The CTA's first minimum per block goes to the global
-// argmin key with a 64-bit atomicMin -- errors are non-negative, so their bit
-// patterns order like the values, and the low word breaks ties toward the
-// earlier candidate, exactly the reference's strict "<" scan.
+// K2: every partition candidate of modes 1, 3 and 7 (bc7.rs:517-569). Grid:
+// (tile, candidate group); warp w evaluates candidate blockIdx.y*NW+w for
+// the 32 blocks of the tile. The CTA's first minimum per block goes to the
+// global argmin key with a 64-bit atomicMin -- errors are non-negative, so
+// their bit patterns order like the values, and the low word breaks ties
+// toward the earlier candidate, exactly the reference's strict "<" scan.
+// MODE 13 runs modes 1 and 3 together: both take their candidates from the
+// same sorted partition list, so candidate c is the same partition in both,
+// and its unquantised endpoints (segment_part2) are computed once for the
+// two.
 template <int MODE, int NW>
 __global__ void __launch_bounds__(NW * 32, (MODE == 7 ? BCN_SEARCH7_MINB : BCN_SEARCH_MINB) * 8 / NW)
     bc7_search_kernel(Work w) {
-    constexpr int mi = MODE == 0 ? 0 : (MODE == 2 ? 1 : (MODE == 1 ? 2 : (MODE == 3 ? 3 : 4)));
-    constexpr bool two = ModeTraits<MODE>::pairs == 2;
+    static_assert(MODE == 1 || MODE == 3 || MODE == 7 || MODE == 13, "two-subset modes");
+    constexpr int CH = MODE == 7 ? 4 : 3;
+    constexpr int mia = MODE == 3 ? 3 : (MODE == 7 ? 4 : 2);  // candidate-mode index (mode 1 for 13)
+    constexpr int NK = MODE == 13 ? 2 : 1;
     __shared__ float px[PX_ROWS][NB];
-    __shared__ float full[two ? 15 : 1][NB];
-    __shared__ unsigned long long best[NW][NB];
+    __shared__ float full[15][NB];
+    __shared__ unsigned long long best[NK][NW][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
     const Plan P = make_plan(w.S);
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
     const Blk blk{&px[0][lane]};
-    // the whole block's statistics (two subsets), one entry per warp at a
-    // time, and the channel square sums
-    if (two)
-        for (int e = warp; e < 15; e += NW) full[e][lane] = stat_entry<ModeTraits<MODE>::ch>(blk, e);
+    // the whole block's statistics, one entry per warp at a time, and the
+    // channel square sums
+    for (int e = warp; e < 15; e += NW) full[e][lane] = stat_entry<CH>(blk, e);
     stage_channel_squares(px, threadIdx.x, NW * 32);
     __syncthreads();
     const int c = blockIdx.y * NW + warp;
-    unsigned long long key = ~0ull;
-    if (c < P.count[mi] && tile_loc(w, tile).valid(lane)) {
-        int qep[24];
-        uint32_t q0, q1;
-        // modes 0 and 2 search partition c for every block of the tile
-        float err = eval_part<MODE, (mi <= 1)>(blk, kPartitionMap, part_of(w, mi, c, gi, P), qep, q0, q1,
-                                    two ? &full[0][lane] : nullptr);
-        if (err == err) key = ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c;
+    const int na = P.count[mia], nb = MODE == 13 ? P.count[3] : 0;
+    unsigned long long key[NK];
+#pragma unroll
+    for (int i = 0; i < NK; i++) key[i] = ~0ull;
+    auto key_of = [&](float err) {
+        return err == err ? ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c : ~0ull;
+    };
+    if (c < max(na, nb) && tile_loc(w, tile).valid(lane)) {
+        const uint32_t pattern = kPartitionMap[part_of(w, mia, c, gi, P)];
+        float ep[16];
+        segment_part2<CH>(blk, pattern, &full[0][lane], ep);
+        if (MODE == 13) {
+            if (c < nb) {
+                float e3[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) e3[i] = ep[i];
+                key[NK - 1] = key_of(quant_fit_part2<3>(blk, pattern, e3));
+            }
+            if (c < na) key[0] = key_of(quant_fit_part2<1>(blk, pattern, ep));
+        } else {
+            key[0] = key_of(quant_fit_part2<MODE>(blk, pattern, ep));
+        }
     }
-    best[warp][lane] = key;
+#pragma unroll
+    for (int i = 0; i < NK; i++) best[i][warp][lane] = key[i];
     __syncthreads();
-    if (warp == 0) {
-        unsigned long long k = best[0][lane];
-        for (int i = 1; i < NW; i++) k = min(k, best[i][lane]);
+    if (warp < NK) {
+        const int mi = warp == 0 ? mia : 3;
+        unsigned long long k = best[warp][0][lane];
+        for (int i = 1; i < NW; i++) k = min(k, best[warp][i][lane]);
         if (k != ~0ull && scratch_ok(w, mi, 5, gi)) atomicMin(&w.keys[(size_t)mi * w.npad + gi], k);
     }
+}
+
+// The distinct pixel subsets of the first NPART three-subset partitions
+// (modes 0 and 2 search partitions 0..15 and 0..63 of that table), in order
+// of first appearance, and each partition's three subsets as indices into
+// that list: 36 distinct subsets among the 48 of mode 0, 140 among the 192
+// of mode 2.
+constexpr uint32_t kPartitionMapHost[128] = {BCN_PARTITION_MAP_VALUES};
+
+template <int NPART>
+struct Subsets3 {
+    static constexpr int kMax = 3 * NPART;
+    uint16_t mask[kMax];
+    uint8_t idx[NPART][3];
+    int count;
+};
+
+template <int NPART>
+constexpr Subsets3<NPART> make_subsets3() {
+    Subsets3<NPART> t{};
+    t.count = 0;
+    for (int p = 0; p < NPART; p++) {
+        for (int j = 0; j < 3; j++) {
+            uint32_t m = 0;
+            for (int k = 0; k < 16; k++)
+                if (((kPartitionMapHost[64 + p] >> (2 * k)) & 3u) == (uint32_t)j) m |= 1u << k;
+            int u = 0;
+            while (u < t.count && t.mask[u] != m) u++;
+            if (u == t.count) t.mask[t.count++] = (uint16_t)m;
+            t.idx[p][j] = (uint8_t)u;
+        }
+    }
+    return t;
+}
+
+constexpr Subsets3<16> kSubsets0Host = make_subsets3<16>();
+constexpr Subsets3<64> kSubsets2Host = make_subsets3<64>();
+static_assert(kSubsets0Host.count == 36 && kSubsets2Host.count == 140, "distinct subsets of modes 0 / 2");
+__constant__ Subsets3<16> kSubsets0 = make_subsets3<16>();
+__constant__ Subsets3<64> kSubsets2 = make_subsets3<64>();
+
+// K2 for modes 0 and 2 (bc7.rs:517-569 over partitions 0..count-1 in table
+// order). One CTA per tile: the warps evaluate the mode's distinct subsets
+// (eval_subset, one subset for the tile's 32 blocks per warp at a time),
+// then each partition's error is the sum of its three subsets' errors plus
+// the block's v . v -- exact integers below 2^24, so the same float as the
+// reference's pixel-order sum -- and the first minimum over the partitions
+// goes to the argmin key.
+template <int MODE, int NW>
+__global__ void __launch_bounds__(NW * 32, BCN_SEARCH3_MINB) bc7_search3_kernel(Work w) {
+    constexpr int mi = MODE == 0 ? 0 : 1;
+    constexpr int NPART = MODE == 0 ? 16 : 64, NS = MODE == 0 ? 36 : 140;
+    const Subsets3<NPART>& T = *(MODE == 0 ? (const Subsets3<NPART>*)&kSubsets0 : (const Subsets3<NPART>*)&kSubsets2);
+    __shared__ float px[PX_ROWS][NB];
+    __shared__ int serr[NS][NB];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x, gi = tile * NB + lane;
+    const Plan P = make_plan(w.S);
+    stage_tile(px, w, tile, threadIdx.x, NW * 32);
+    __syncthreads();
+    stage_channel_squares(px, threadIdx.x, NW * 32);
+    __syncthreads();
+    const Blk blk{&px[0][lane]};
+    const int count = min(P.count[mi], NPART);
+    const bool valid = tile_loc(w, tile).valid(lane);
+    for (int u = warp; u < NS; u += NW) serr[u][lane] = valid ? eval_subset<MODE>(blk, T.mask[u]) : 0;
+    __syncthreads();
+    if (warp != 0 || !valid || count == 0) return;
+    const int v2 = block_sq<3>(blk);
+    unsigned long long key = ~0ull;
+    for (int c = 0; c < count; c++) {
+        const int total = serr[T.idx[c][0]][lane] + serr[T.idx[c][1]][lane] + serr[T.idx[c][2]][lane] + v2;
+        key = min(key, ((unsigned long long)__float_as_uint((float)total) << 32) | (uint32_t)c);
+    }
+    if (scratch_ok(w, mi, 5, gi)) atomicMin(&w.keys[(size_t)mi * w.npad + gi], key);
 }
 
 // K3: refinement of each block's winning partition + coding (bc7.rs:571-609).
@@ -628,25 +733,23 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
         if (w.S.channels == 3) bc7_mode6_kernel<3, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
         else bc7_mode6_kernel<4, NWR><<<rgrid, NWR * 32, 0, s2>>>(w, ntiles);
     }
-    auto search = [&](int mi, cudaStream_t st) {
-        const int mode = mi == 0 ? 0 : (mi == 1 ? 2 : (mi == 2 ? 1 : (mi == 3 ? 3 : 7)));
+    // K2 of modes 1/3/7; mode 13 = modes 1 and 3 in one launch
+    auto search = [&](int mode, int count, cudaStream_t st) {
         // 4 candidates per CTA when 8 would leave a last group at most half
         // full (e.g. 12 candidates: 3 full CTAs of 4 instead of 8 + 4)
-        const int rem = P.count[mi] % 8;
+        const int rem = count % 8;
         if (search_warps == 4 || (rem != 0 && rem <= 4)) {
-            dim3 g(ntiles, groups(P.count[mi], 4));
+            dim3 g(ntiles, groups(count, 4));
             switch (mode) {
-                case 0: bc7_search_kernel<0, 4><<<g, 128, 0, st>>>(w); break;
-                case 2: bc7_search_kernel<2, 4><<<g, 128, 0, st>>>(w); break;
+                case 13: bc7_search_kernel<13, 4><<<g, 128, 0, st>>>(w); break;
                 case 1: bc7_search_kernel<1, 4><<<g, 128, 0, st>>>(w); break;
                 case 3: bc7_search_kernel<3, 4><<<g, 128, 0, st>>>(w); break;
                 default: bc7_search_kernel<7, 4><<<g, 128, 0, st>>>(w); break;
             }
         } else {
-            dim3 g(ntiles, groups(P.count[mi], 8));
+            dim3 g(ntiles, groups(count, 8));
             switch (mode) {
-                case 0: bc7_search_kernel<0, 8><<<g, 256, 0, st>>>(w); break;
-                case 2: bc7_search_kernel<2, 8><<<g, 256, 0, st>>>(w); break;
+                case 13: bc7_search_kernel<13, 8><<<g, 256, 0, st>>>(w); break;
                 case 1: bc7_search_kernel<1, 8><<<g, 256, 0, st>>>(w); break;
                 case 3: bc7_search_kernel<3, 8><<<g, 256, 0, st>>>(w); break;
                 default: bc7_search_kernel<7, 8><<<g, 256, 0, st>>>(w); break;
@@ -654,27 +757,37 @@ static cudaError_t run_pipeline(Work& w, uint32_t ntiles, void* scratch, int sea
         }
     };
     // modes 0 and 2 search partitions in table order: no prep needed
-    if (P.count[0]) search(0, s3);
-    if (P.count[1]) search(1, s3);
+    constexpr int NW3 = BCN_SEARCH3_WARPS;
+    if (P.count[0]) bc7_search3_kernel<0, NW3><<<ntiles, NW3 * 32, 0, s3>>>(w);
+    if (P.count[1]) bc7_search3_kernel<2, NW3><<<ntiles, NW3 * 32, 0, s3>>>(w);
     if (P.count[0]) bc7_refine_kernel<0, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
     if (P.count[1]) bc7_refine_kernel<2, NWR><<<rgrid, NWR * 32, 0, s3>>>(w, ntiles);
     bc7_prep_kernel<NWP><<<ntiles, NWP * 32, 0, s>>>(w);
     // modes 1/3/7: each refine starts on a fourth stream as soon as its own
     // search is done, overlapping the next searches (the refine kernels are
-    // latency-bound at 16 warps per SM)
+    // latency-bound at 16 warps per SM). Modes 1 and 3 search together.
     const bool split = s2 != s;
-    for (int mi = 2; mi < 5; mi++) {
-        if (!P.count[mi]) continue;
-        search(mi, s);
-        if (split) {
-            cudaError_t e = cudaEventRecord(t_side.searched[mi - 2], s);
-            if (e != cudaSuccess) return e;
-            if ((e = cudaStreamWaitEvent(t_side.st3, t_side.searched[mi - 2], 0)) != cudaSuccess) return e;
-        }
-        cudaStream_t sr = split ? t_side.st3 : s;
-        if (mi == 2) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
-        else if (mi == 3) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
-        else bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+    auto after_search = [&](int ev) -> cudaError_t {
+        if (!split) return cudaSuccess;
+        cudaError_t e = cudaEventRecord(t_side.searched[ev], s);
+        if (e != cudaSuccess) return e;
+        return cudaStreamWaitEvent(t_side.st3, t_side.searched[ev], 0);
+    };
+    cudaStream_t sr = split ? t_side.st3 : s;
+    if (P.count[2] || P.count[3]) {
+        if (P.count[2] && P.count[3]) search(13, max(P.count[2], P.count[3]), s);
+        else if (P.count[2]) search(1, P.count[2], s);
+        else search(3, P.count[3], s);
+        cudaError_t e = after_search(0);
+        if (e != cudaSuccess) return e;
+        if (P.count[2]) bc7_refine_kernel<1, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+        if (P.count[3]) bc7_refine_kernel<3, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
+    }
+    if (P.count[4]) {
+        search(7, P.count[4], s);
+        cudaError_t e = after_search(1);
+        if (e != cudaSuccess) return e;
+        bc7_refine_kernel<7, NWR><<<rgrid, NWR * 32, 0, sr>>>(w, ntiles);
     }
     if (split) {
         cudaError_t e = cudaEventRecord(t_side.join, s2);

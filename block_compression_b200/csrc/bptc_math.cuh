@@ -15,11 +15,27 @@ constexpr int NB = 32;  // blocks per tile; lane l of each warp owns block l
 // and PX_SQ.. (per channel, the sum of the squares of its 16 values), which
 // the integer index fit reads through packed() and sq().
 constexpr int PX_PACKED = 64, PX_SQ = 80, PX_ROWS = 84;
+
+// Transposes four pixel words (4 channel bytes each) into four channel words
+// (the 4 pixels' bytes of one channel each): c[ch] byte i = w_i byte ch.
+BCN_DEV void transpose_bytes4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t c[4]) {
+    const uint32_t t0 = __byte_perm(w0, w1, 0x5140), t1 = __byte_perm(w2, w3, 0x5140);
+    const uint32_t t2 = __byte_perm(w0, w1, 0x7362), t3 = __byte_perm(w2, w3, 0x7362);
+    c[0] = __byte_perm(t0, t1, 0x5410);
+    c[1] = __byte_perm(t0, t1, 0x7632);
+    c[2] = __byte_perm(t2, t3, 0x5410);
+    c[3] = __byte_perm(t2, t3, 0x7632);
+}
+
 struct Blk {
     const float* p;
     BCN_DEV float operator()(int c, int k) const { return p[(c * 16 + k) * NB]; }
     BCN_DEV uint32_t packed(int k) const { return __float_as_uint(p[(PX_PACKED + k) * NB]); }
     BCN_DEV int sq(int c) const { return __float_as_int(p[(PX_SQ + c) * NB]); }
+    // channels 0-3 of pixels 4g..4g+3, one byte per pixel
+    BCN_DEV void group_bytes(int g, uint32_t c[4]) const {
+        transpose_bytes4(packed(4 * g), packed(4 * g + 1), packed(4 * g + 2), packed(4 * g + 3), c);
+    }
 };
 
 // ---- shared math (src/encode/common.rs) -------------------------------------
@@ -494,54 +510,63 @@ BCN_DEV float block_quant(const B& blk, const float* ep, uint32_t pattern, uint3
     return total;
 }
 
-// block_quant<CH, BITS, PAIRS, true> walking each subset's pixels in turn,
-// with that pair's values in registers instead of selected per pixel. The
-// per-pixel arithmetic is the same; the pixel errors are integers (squared
-// differences of bytes, at most 16 * 4 * 255^2 in total, below 2^24), so
-// their float sum is exact in any order and equals the pixel-order sum.
-// Meant for a pattern shared by the whole warp (no divergent loops).
-template <int CH, int BITS, int PAIRS, class B>
-BCN_DEV float block_quant_by_subset(const B& blk, const float* ep, uint32_t pattern, uint32_t& q0, uint32_t& q1) {
-    int total = 0;
-    q0 = 0;
-    q1 = 0;
-#pragma unroll
-    for (int j = 0; j < PAIRS; j++) {
-        const FitPair f = fit_pair<CH>(ep + 8 * j);
-        const uint32_t mask = PAIRS == 1 ? 0xFFFFu : subset_mask_from_map(pattern, j);
-        for (uint32_t m = mask; m; m &= m - 1) {
-            const int k = __ffs(m) - 1;
-            int be;
-            const uint32_t bq = fit_pixel_pk<BITS>(blk.packed(k), f, be);
-            if (k < 8) q0 |= bq << (4 * k);
-            else q1 |= bq << (4 * (k - 8));
-            total += be;
-        }
-    }
-    return (float)(total + block_sq<CH>(blk));
-}
-
 // common.rs:142-205. Writes ep[0..CH) and ep[4..4+CH). INT: 8-bit pixels
 // (the sums of index and pixel products are exact integers, see mac).
+// INT: 8-bit pixels, so every sum is an exact integer below 2^24, in any
+// order: they are taken four pixels at a time as byte dot products of the
+// channel bytes (group_bytes), the index bytes and the subset's pixel mask
+// bytes, and converted to float once (the same values as the reference's
+// float sums).
 template <int CH, int BITS, bool INT = false, class B>
 BCN_DEV void opt_endpoints(float* ep, const B& blk, uint32_t q0, uint32_t q1, uint32_t mask) {
     constexpr int levels = 1 << BITS;
     const float lm1 = (float)(levels - 1);
     float atb1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, sum[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float sum_q = 0.0f, sum_qq = 0.0f;
+    if constexpr (INT) {
+        uint32_t sq = 0, sqq = 0, sc[4] = {0, 0, 0, 0}, at[4] = {0, 0, 0, 0};
+        const uint32_t lmb = (uint32_t)(levels - 1) * 0x01010101u;
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
-        float q = (float)(((k < 8 ? q0 : q1) >> (4 * (k & 7))) & 15);
-        if (((mask >> k) & 1) == 0) continue;
-        float x = lm1 - q;
-        sum_q += q;
-        sum_qq = mac<INT>(sum_qq, q, q);
-        sum[4] += 1.0f;
+        for (int g = 0; g < 4; g++) {
+            uint32_t c[4];
+            blk.group_bytes(g, c);
+            // index bytes of pixels 4g..4g+3 (nibbles of q0 / q1)
+            const uint32_t h = (g < 2 ? q0 : q1) >> (16 * (g & 1));
+            const uint32_t qb = __byte_perm(h & 0x0F0Fu, (h >> 4) & 0x0F0Fu, 0x5140);
+            // mask bit of pixel 4g+i -> byte i (0 or 1), and 0 / 0xFF
+            const uint32_t mb = (((mask >> (4 * g)) & 0xFu) * 0x00204081u) & 0x01010101u, mf = mb * 0xFFu;
+            const uint32_t xb = (lmb - qb) & mf;  // bytes lm1 - q of the subset's pixels
+            sq = __dp4a(qb, mb, sq);
+            sqq = __dp4a(qb & mf, qb, sqq);
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                sc[p] = __dp4a(c[p], mb, sc[p]);
+                at[p] = __dp4a(c[p], xb, at[p]);
+            }
+        }
+        sum_q = (float)sq;
+        sum_qq = (float)sqq;
+        sum[4] = (float)__popc(mask & 0xFFFFu);
 #pragma unroll
         for (int p = 0; p < CH; p++) {
-            float v = blk(p, k);
-            sum[p] += v;
-            atb1[p] = mac<INT>(atb1[p], x, v);
+            sum[p] = (float)sc[p];
+            atb1[p] = (float)at[p];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            float q = (float)(((k < 8 ? q0 : q1) >> (4 * (k & 7))) & 15);
+            if (((mask >> k) & 1) == 0) continue;
+            float x = lm1 - q;
+            sum_q += q;
+            sum_qq += q * q;
+            sum[4] += 1.0f;
+#pragma unroll
+            for (int p = 0; p < CH; p++) {
+                float v = blk(p, k);
+                sum[p] += v;
+                atb1[p] += x * v;
+            }
         }
     }
     float atb2[4];
