@@ -429,9 +429,59 @@ static_assert(kSubsets0Host.count == 36 && kSubsets2Host.count == 140, "distinct
 __constant__ Subsets3<16> kSubsets0 = make_subsets3<16>();
 __constant__ Subsets3<64> kSubsets2 = make_subsets3<64>();
 
+// Which warp of a CTA of NW evaluates which distinct subset: longest first,
+// each to the warp with the least work so far, at an estimated cost of
+// 300 + 70 * (pixels) instructions per subset (a fixed endpoint fit plus
+// per-pixel statistics, projection and index fit). Subsets of 1 to 14
+// pixels differ in cost by about 3x, and the CTA waits for its slowest warp
+// before the partition sums. order[start[w] .. start[w + 1]) are warp w's
+// subsets.
+template <int NPART, int NW>
+struct SubsetSchedule {
+    uint8_t order[3 * NPART];
+    uint8_t start[NW + 1];
+};
+
+template <int NPART, int NW>
+constexpr SubsetSchedule<NPART, NW> make_schedule(const Subsets3<NPART>& t) {
+    SubsetSchedule<NPART, NW> r{};
+    int owner[3 * NPART] = {};
+    bool done[3 * NPART] = {};
+    int load[NW] = {};
+    for (int n = 0; n < t.count; n++) {
+        int best = -1, bc = -1;
+        for (int u = 0; u < t.count; u++) {
+            int pc = 0;
+            for (uint32_t m = t.mask[u]; m; m &= m - 1) pc++;
+            if (!done[u] && 300 + 70 * pc > bc) {
+                bc = 300 + 70 * pc;
+                best = u;
+            }
+        }
+        int w = 0;
+        for (int i = 1; i < NW; i++)
+            if (load[i] < load[w]) w = i;
+        done[best] = true;
+        owner[best] = w;
+        load[w] += bc;
+    }
+    int pos = 0;
+    for (int w = 0; w < NW; w++) {
+        r.start[w] = (uint8_t)pos;
+        for (int u = 0; u < t.count; u++)
+            if (owner[u] == w) r.order[pos++] = (uint8_t)u;
+    }
+    r.start[NW] = (uint8_t)pos;
+    return r;
+}
+
+__constant__ SubsetSchedule<16, BCN_SEARCH3_WARPS> kSchedule0 = make_schedule<16, BCN_SEARCH3_WARPS>(kSubsets0Host);
+__constant__ SubsetSchedule<64, BCN_SEARCH3_WARPS> kSchedule2 = make_schedule<64, BCN_SEARCH3_WARPS>(kSubsets2Host);
+
 // K2 for modes 0 and 2 (bc7.rs:517-569 over partitions 0..count-1 in table
 // order). One CTA per tile: the warps evaluate the mode's distinct subsets
-// (eval_subset, one subset for the tile's 32 blocks per warp at a time),
+// (eval_subset, one subset for the tile's 32 blocks per warp at a time, in
+// the order of the subset schedule),
 // then each partition's error is the sum of its three subsets' errors plus
 // the block's v . v -- exact integers below 2^24, so the same float as the
 // reference's pixel-order sum -- and the first minimum over the partitions
@@ -453,7 +503,13 @@ __global__ void __launch_bounds__(NW * 32, BCN_SEARCH3_MINB) bc7_search3_kernel(
     const Blk blk{&px[0][lane]};
     const int count = min(P.count[mi], NPART);
     const bool valid = tile_loc(w, tile).valid(lane);
-    for (int u = warp; u < NS; u += NW) serr[u][lane] = valid ? eval_subset<MODE>(blk, T.mask[u]) : 0;
+    static_assert(NW == BCN_SEARCH3_WARPS, "the subset schedules are made for BCN_SEARCH3_WARPS warps");
+    const SubsetSchedule<NPART, NW>& S =
+        *(MODE == 0 ? (const SubsetSchedule<NPART, NW>*)&kSchedule0 : (const SubsetSchedule<NPART, NW>*)&kSchedule2);
+    for (int i = S.start[warp]; i < S.start[warp + 1]; i++) {
+        const int u = S.order[i];
+        serr[u][lane] = valid ? eval_subset<MODE>(blk, T.mask[u]) : 0;
+    }
     __syncthreads();
     if (warp != 0 || !valid || count == 0) return;
     const int v2 = block_sq<3>(blk);
