@@ -240,6 +240,17 @@ BCN_DEV float opaque_err(const B& blk, uint32_t channels) {
     return e;
 }
 
+// The smaller subset (pixel mask) of a two-subset partition. A partition's
+// bound is the sum of its two subsets' bounds, computed from one subset's
+// statistics and the whole block's minus them (exact integers either way);
+// the sum is the same whichever subset comes first (float addition is
+// commutative), so the loop over pixels runs over the smaller subset: 6.4
+// pixels on average over the 64 partitions instead of 8.7 for subset 0.
+BCN_DEV uint32_t smaller_subset(uint32_t pattern) {
+    const uint32_t m0 = subset_mask_from_map(pattern, 0);
+    return __popc(m0) <= 8 ? m0 : ~m0 & 0xFFFFu;
+}
+
 // K1: PCA split bounds + ascending top-k partition lists (bc7.rs:622-655,
 // 819-851; common.rs:126-140).
 template <int NW>
@@ -260,7 +271,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
         stats_masked<4, true>(blk, 0xFFFFu, full);
         for (int part = warp; part < 64; part += NW) {
             float st[15], cv[10];
-            stats_masked<4, true>(blk, subset_mask_from_map(kPartitionMap[part], 0), st);
+            stats_masked<4, true>(blk, smaller_subset(kPartitionMap[part]), st);
             covar_from_stats<4, true>(cv, st);
             float ba = 0.0f, bb = 0.0f;
             ba += pca_bound<3>(cv);
@@ -279,7 +290,7 @@ __global__ void __launch_bounds__(NW * 32, BCN_PREP_MINB) bc7_prep_kernel(Work w
         if (set == 0) stats_masked<3, true>(blk, 0xFFFFu, full);
         else stats_masked<4, true>(blk, 0xFFFFu, full);
         for (int part = warp; part < 64; part += NW) {
-            uint32_t mask = subset_mask_from_map(kPartitionMap[part], 0);
+            uint32_t mask = smaller_subset(kPartitionMap[part]);
             float b12 = set == 0 ? pca_bound_split<3, true>(blk, mask, full) : pca_bound_split<4, true>(blk, mask, full);
             keys[set][part][lane] = part + (int)b12 * 64;
         }
