@@ -55,7 +55,7 @@ using namespace bptc;
 #define BCN_BC6H_PREP_MINB 4
 #endif
 #ifndef BCN_BC6H_SEARCH_MINB
-#define BCN_BC6H_SEARCH_MINB 5
+#define BCN_BC6H_SEARCH_MINB 6  // 80 registers: 0.242 ms at 1024x1024, 96 (5) 0.246, 64 (8) 0.246
 #endif
 #ifndef BCN_BC6H_REFINE_MINB
 #define BCN_BC6H_REFINE_MINB 4
@@ -702,12 +702,16 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_PREP_MINB) bc6h_prep_kernel(
     }
 }
 
-// K2: candidate `blockIdx.y * NW + warp` = (two-region encode j, list entry
-// c) for the 32 blocks of the tile (bc6h_enc_2p_part_fast, bc6h.rs:304-324).
-// A candidate counts only with an error below +inf (the reference's running
-// best starts there, bc6h.rs:337); errors are non-negative, so the argmin
-// key's high word orders like the error and the low word keeps the earliest
-// candidate among equal errors, the reference's strict "<" scan.
+// K2: list entry c = `blockIdx.y * NW + warp` for the 32 blocks of the tile,
+// for every two-region encode j (bc6h_enc_2p_part_fast, bc6h.rs:304-324).
+// Entry c is the same partition for every j (one list per block), and its
+// unquantised endpoints (block_segment of both subsets) depend only on the
+// pixels, so they are computed once and each encode quantises its own copy
+// with its endpoint precision and bounds. A candidate counts only with an
+// error below +inf (the reference's running best starts there,
+// bc6h.rs:337); errors are non-negative, so the argmin key's high word
+// orders like the error and the low word keeps the earliest candidate among
+// equal errors, the reference's strict "<" scan.
 __global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_kernel(Work w) {
     __shared__ float px[48][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -715,17 +719,32 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_ker
     const Plan P = make_plan(w.S);
     stage_tile(px, w, tile, threadIdx.x, NW * 32);
     __syncthreads();
-    const int item = blockIdx.y * NW + warp;
-    if (item >= P.n2 * P.k || gi >= w.nblocks) return;
-    const int j = item / P.k, c = item - j * P.k;
-    if (!scratch_ok(w, j, P.n2, gi) || !scratch_ok(w, c, P.k, gi)) return;
-    const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
+    const int c = blockIdx.y * NW + warp;
+    if (c >= P.k || gi >= w.nblocks || !scratch_ok(w, c, P.k, gi)) return;
     const Blk blk{&px[0][lane]};
-    int qep[24];
-    uint32_t q0, q1;
-    const float err = eval_2p(blk, w.lists[(size_t)c * w.npad + gi] & 31, st.epb, st.qb, qep, q0, q1);
-    if (err < __int_as_float(0x7f800000))
-        atomicMin(&w.keys[(size_t)j * w.npad + gi], ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c);
+    const uint32_t pattern = kPartitionMap[w.lists[(size_t)c * w.npad + gi] & 31];
+    float ep0[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) ep0[i] = 0.0f;
+#pragma unroll
+    for (int h = 0; h < 2; h++) block_segment<3, false>(blk, subset_mask_from_map(pattern, h), ep0 + 8 * h);
+#pragma unroll 1
+    for (int j = 0; j < P.n2; j++) {
+        if (!scratch_ok(w, j, P.n2, gi)) continue;
+        const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
+        float ep[24];
+        int qep[24];
+#pragma unroll
+        for (int i = 0; i < 24; i++) {
+            ep[i] = i < 16 ? ep0[i] : 0.0f;
+            qep[i] = 0;
+        }
+        uint32_t q0, q1;
+        quant_dequant<2>(qep, ep, st.epb, st.qb);
+        const float err = block_quant<3, 3, 2>(blk, ep, pattern, q0, q1);
+        if (err < __int_as_float(0x7f800000))
+            atomicMin(&w.keys[(size_t)j * w.npad + gi], ((unsigned long long)__float_as_uint(err) << 32) | (uint32_t)c);
+    }
 }
 
 // K3: the winner of two-region encode blockIdx.y, refined (bc6h.rs:355-387);
@@ -922,7 +941,7 @@ cudaError_t launch_bc6h_encode(const void* src, size_t stride_bytes, int source_
     if (P.n > P.n2)
         bc6h_enc1_kernel<<<dim3((ntiles + NW - 1) / NW, (uint32_t)(P.n - P.n2)), NW * 32, 0, s1>>>(w, ntiles, P.n2);
     if (P.n2 > 0) {
-        const uint32_t groups = (uint32_t)(P.n2 * P.k + NW - 1) / NW;
+        const uint32_t groups = (uint32_t)(P.k + NW - 1) / NW;
         bc6h_search_kernel<<<dim3(ntiles, groups), NW * 32, 0, s>>>(w);
         bc6h_refine2_kernel<<<dim3((ntiles + NW - 1) / NW, (uint32_t)P.n2), NW * 32, 0, s>>>(w, ntiles);
     }
