@@ -429,9 +429,8 @@ static int enqueue_band(int variant, const void* settings, const uint8_t* src, u
 
 // Host-buffer encode, pipelined: the image is cut into bands of whole block
 // rows (about 2 MiB of source for the first, 8 MiB for the others) and band
-// i's upload, encode and download
-// run on three streams, so the copies of one band overlap the kernels of its
-// neighbours. Blocks are independent and every band but the last is a whole
+// i's upload, encode and download run on three streams, so the copies of one
+// band overlap the kernels of its neighbours. Blocks are independent and every band but the last is a whole
 // number of block rows, so the bands' blocks are exactly the image's.
 static int host_encode(int variant, const void* settings, const uint8_t* src, size_t stride_bytes, size_t bpp,
                        uint8_t* blocks, uint32_t width, uint32_t height, int bc6h_source) {
