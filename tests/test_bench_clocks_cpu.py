@@ -47,9 +47,12 @@ def test_nvidia_smi_lines_are_the_fallback():
 
 def test_bc7_kernel_count_matches_the_pipeline():
     from block_compression_b200.settings import BC7Settings
-    # alpha_basic: prep, searches and refines of modes 0, 1, 3 and 7 (mode 2
-    # skipped), three mode-4/5 launches, mode 6, select -- the 14 BC7 kernels
-    # of the benchmark's launch list
-    assert bench.bc7_kernel_count(BC7Settings.alpha_basic()) == 14
+    # alpha_basic: prep, the searches of mode 0, modes 1+3 (one launch) and
+    # mode 7 (mode 2 skipped), the refines of modes 0, 1, 3 and 7, three
+    # mode-4/5 launches, mode 6, select -- the 13 BC7 kernels of the
+    # benchmark's launch list
+    assert bench.bc7_kernel_count(BC7Settings.alpha_basic()) == 13
     # opaque_basic: no mode 7 candidates
-    assert bench.bc7_kernel_count(BC7Settings.opaque_basic()) == 12
+    assert bench.bc7_kernel_count(BC7Settings.opaque_basic()) == 11
+    # opaque_slow: mode 2 searched too
+    assert bench.bc7_kernel_count(BC7Settings.opaque_slow()) == 13
