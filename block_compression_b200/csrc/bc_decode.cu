@@ -64,8 +64,13 @@ BCN_DEV uint32_t cta_sort_slot(uint32_t key, uint32_t nkeys, uint32_t* s_cnt) {
 #ifndef BCN_BC7DEC_ITEMS
 #define BCN_BC7DEC_ITEMS 4
 #endif
+// Resident CTAs of 256 threads per SM asked of the register allocator: 4
+// (63 registers, no spill) hides the sort's barriers behind 32 warps; left
+// to itself the compiler takes 99 registers and 2 CTAs, 22-28% slower at
+// 8192x8192 (mode-6 image 77% of HBM at 4 CTAs, 60% at 2; mixed modes 52%
+// and 43%).
 #ifndef BCN_BC7DEC_MINB
-#define BCN_BC7DEC_MINB 1
+#define BCN_BC7DEC_MINB 4
 #endif
 constexpr int kSortItems = BCN_BC7DEC_ITEMS;
 
@@ -130,14 +135,19 @@ __global__ void __launch_bounds__(kSortCta, BCN_BC7DEC_MINB) bc7_decode_sorted_k
             uint4 b = s_blk[q * kSortCta + t];
             uint32_t i = s_orig[q * kSortCta + t];
             if (i < n) {
-                uint32_t px[16];
-                decode_bc7_block((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32), px);
                 uint32_t by = i / bw, bx = i - by * bw;
                 if (!BCN_GUARD(by, bh, CHECK_DECODE_STORE)) continue;
-#pragma unroll
-                for (int y = 0; y < 4; y++)
-                    *reinterpret_cast<uint4*>(out + (size_t)(by * 4 + y) * pitch + (size_t)bx * 16) =
-                        make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+                uint8_t* o = out + (size_t)(by * 4) * pitch + (size_t)bx * 16;
+                // each texel row is stored as soon as its 4 texels exist
+                // (4 live texel registers instead of 16)
+                uint32_t row[4];
+                decode_bc7_each((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32),
+                                [&](int k, uint32_t px) {
+                                    row[k & 3] = px;
+                                    if ((k & 3) == 3)
+                                        *reinterpret_cast<uint4*>(o + (size_t)(k >> 2) * pitch) =
+                                            make_uint4(row[0], row[1], row[2], row[3]);
+                                });
             }
         }
         __syncthreads();  // s_blk / s_orig / s_cnt are reused by the next group
