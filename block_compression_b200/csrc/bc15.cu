@@ -356,10 +356,10 @@ BCN_DEV void decode_bc15_rgba8(int variant, const uint32_t* w, uint32_t out[16])
     }
 }
 
-template <int VARIANT>
 // 12 resident CTAs per SM (40 registers, no spill) keep more block reads in
 // flight than the compiler's 48 registers: BC1 85% instead of 82% of HBM at
 // 8192x8192, BC3 76% instead of 74%, BC5 81% instead of 79%.
+template <int VARIANT>
 __global__ void __launch_bounds__(128, 12) bc15_decode_kernel(const uint8_t* __restrict__ blocks, uint32_t bw, uint32_t bh,
                                                            uint8_t* __restrict__ out, size_t pitch, bool aligned) {
     constexpr int words = (VARIANT == BC_BC1 || VARIANT == BC_BC4) ? 2 : 4;
