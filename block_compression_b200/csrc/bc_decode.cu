@@ -64,13 +64,13 @@ BCN_DEV uint32_t cta_sort_slot(uint32_t key, uint32_t nkeys, uint32_t* s_cnt) {
 #ifndef BCN_BC7DEC_ITEMS
 #define BCN_BC7DEC_ITEMS 4
 #endif
-// Resident CTAs of 256 threads per SM asked of the register allocator: 4
-// (63 registers, no spill) hides the sort's barriers behind 32 warps; left
-// to itself the compiler takes 99 registers and 2 CTAs, 22-28% slower at
-// 8192x8192 (mode-6 image 77% of HBM at 4 CTAs, 60% at 2; mixed modes 52%
-// and 43%).
+// Resident CTAs of 256 threads per SM asked of the register allocator: 6
+// (40 registers, no spill) hides the sort's barriers behind 48 warps. At
+// 8192x8192 the mode-6 image decodes at 81% of HBM with 6 CTAs, 80% with 5,
+// 76% with 4 and 60% with the compiler's own choice (99 registers, 2 CTAs);
+// mixed modes at 54.5%, 54%, 52% and 43%. 7 and 8 spill.
 #ifndef BCN_BC7DEC_MINB
-#define BCN_BC7DEC_MINB 4
+#define BCN_BC7DEC_MINB 6
 #endif
 constexpr int kSortItems = BCN_BC7DEC_ITEMS;
 
