@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(kSortCta, BCN_BC7DEC_MINB) bc7_decode_sorted_k
     __shared__ uint4 s_blk[G];
     __shared__ uint32_t s_orig[G];
     __shared__ uint32_t s_cnt[32];
+    __shared__ uint32_t s_pal[8][kSortCta];  // per-thread texel palette (decode_bc7_mode)
     const uint32_t n = bw * bh, t = threadIdx.x, lane = t & 31u;
     const uint32_t stride = gridDim.x * G;
     for (uint32_t base = blockIdx.x * G; base < n; base += stride) {
@@ -141,13 +142,14 @@ __global__ void __launch_bounds__(kSortCta, BCN_BC7DEC_MINB) bc7_decode_sorted_k
                 // each texel row is stored as soon as its 4 texels exist
                 // (4 live texel registers instead of 16)
                 uint32_t row[4];
-                decode_bc7_each((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32),
-                                [&](int k, uint32_t px) {
-                                    row[k & 3] = px;
-                                    if ((k & 3) == 3)
-                                        *reinterpret_cast<uint4*>(o + (size_t)(k >> 2) * pitch) =
-                                            make_uint4(row[0], row[1], row[2], row[3]);
-                                });
+                decode_bc7_each<kSortCta>((uint64_t)b.x | ((uint64_t)b.y << 32), (uint64_t)b.z | ((uint64_t)b.w << 32),
+                                          [&](int k, uint32_t px) {
+                                              row[k & 3] = px;
+                                              if ((k & 3) == 3)
+                                                  *reinterpret_cast<uint4*>(o + (size_t)(k >> 2) * pitch) =
+                                                      make_uint4(row[0], row[1], row[2], row[3]);
+                                          },
+                                          &s_pal[0][t]);
             }
         }
         __syncthreads();  // s_blk / s_orig / s_cnt are reused by the next group

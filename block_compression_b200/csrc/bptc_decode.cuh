@@ -97,8 +97,16 @@ BCN_DEV uint32_t bptc_weight(uint32_t i) {
 BCN_DEV uint32_t lerp2(uint32_t e0, uint32_t e1, uint32_t w) { return (e0 * (64u - w) + e1 * w + 0x00200020u) >> 6; }
 
 // emit(k, texel) receives pixel k's RGBA8 texel (R in the low byte).
-template <int MODE, class Emit>
-BCN_DEV void decode_bc7_mode(const uint32_t d[5], Emit&& emit) {
+// PSTRIDE > 0: the caller gives each thread a palette of 8 words at
+// pal[0], pal[PSTRIDE], ..., pal[7 * PSTRIDE] (shared memory, one column per
+// thread). The two-subset modes with 2-bit indices (3 and 7) then form their
+// 4 texels per subset once, with the same arithmetic as the per-pixel path
+// below, and look each pixel's texel up by (subset, index) -- fewer integer
+// instructions per pixel than selecting the subset's endpoints and
+// interpolating 16 times. (Mode 2 would need 12 words; that much shared
+// memory cost the sorted decoder a CTA per SM and measured slower.)
+template <int MODE, int PSTRIDE = 0, class Emit>
+BCN_DEV void decode_bc7_mode(const uint32_t d[5], Emit&& emit, uint32_t* pal = nullptr) {
     constexpr int NS = (MODE == 0 || MODE == 2) ? 3 : ((MODE == 1 || MODE == 3 || MODE == 7) ? 2 : 1);
     constexpr int NEP = 2 * NS;
     constexpr int PB = MODE == 0 ? 4 : (NS > 1 ? 6 : 0);
@@ -173,6 +181,21 @@ BCN_DEV void decode_bc7_mode(const uint32_t d[5], Emit&& emit) {
             da[j] = 0;
         }
     }
+    if constexpr (PSTRIDE > 0 && IB == 2 && IB2 == 0 && NS == 2) {
+#pragma unroll
+        for (int j = 0; j < NS; j++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t w = bptc_weight<2>((uint32_t)i);
+                pal[(4 * j + i) * PSTRIDE] = __byte_perm((brg[j] + drg[j] * w) >> 6, (bba[j] + dba[j] * w) >> 6, 0x6420u);
+            }
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const uint32_t e = ((map >> (2 * k)) & 3u) * 4u + ((uint32_t)(x >> (2 * k)) & 3u);
+            emit(k, pal[e * PSTRIDE]);
+        }
+        return;
+    }
     // rotation: swap alpha with R (1), G (2) or B (3)
     const uint32_t rot_sel = rot == 1 ? 0x0213u : (rot == 2 ? 0x1230u : (rot == 3 ? 0x2310u : 0x3210u));
 #pragma unroll
@@ -213,20 +236,20 @@ BCN_DEV void decode_bc7_mode(const uint32_t d[5], Emit&& emit) {
 
 // Decodes one BC7 block, handing each texel to emit(k, texel); a reserved
 // mode encoding gives 16 zero texels.
-template <class Emit>
-BCN_DEV void decode_bc7_each(uint64_t lo, uint64_t hi, Emit&& emit) {
+template <int PSTRIDE = 0, class Emit>
+BCN_DEV void decode_bc7_each(uint64_t lo, uint64_t hi, Emit&& emit, uint32_t* pal = nullptr) {
     const uint32_t d[5] = {(uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32), 0u};
     uint32_t low = d[0] & 0xFFu;
     int mode = low ? __ffs((int)low) - 1 : 8;
     switch (mode) {
-        case 0: decode_bc7_mode<0>(d, emit); break;
-        case 1: decode_bc7_mode<1>(d, emit); break;
-        case 2: decode_bc7_mode<2>(d, emit); break;
-        case 3: decode_bc7_mode<3>(d, emit); break;
-        case 4: decode_bc7_mode<4>(d, emit); break;
-        case 5: decode_bc7_mode<5>(d, emit); break;
-        case 6: decode_bc7_mode<6>(d, emit); break;
-        case 7: decode_bc7_mode<7>(d, emit); break;
+        case 0: decode_bc7_mode<0, PSTRIDE>(d, emit, pal); break;
+        case 1: decode_bc7_mode<1, PSTRIDE>(d, emit, pal); break;
+        case 2: decode_bc7_mode<2, PSTRIDE>(d, emit, pal); break;
+        case 3: decode_bc7_mode<3, PSTRIDE>(d, emit, pal); break;
+        case 4: decode_bc7_mode<4, PSTRIDE>(d, emit, pal); break;
+        case 5: decode_bc7_mode<5, PSTRIDE>(d, emit, pal); break;
+        case 6: decode_bc7_mode<6, PSTRIDE>(d, emit, pal); break;
+        case 7: decode_bc7_mode<7, PSTRIDE>(d, emit, pal); break;
         default:
 #pragma unroll
             for (int k = 0; k < 16; k++) emit(k, 0u);
