@@ -380,26 +380,27 @@ BCN_DEV void bc6h_pack(uint32_t packed[4], const int* qep, int mode) {
 }
 
 // 2-region candidate (bc6h.rs:304-324)
-BCN_DEV float eval_2p(const Blk& blk, int part_id, int epb, const int qb[6], int qep[24], uint32_t& q0, uint32_t& q1) {
+// ep0: the partition's unquantised endpoints (block_segment of both
+// subsets), as the search computed and kept them.
+BCN_DEV float eval_2p(const Blk& blk, int part_id, const float ep0[16], int epb, const int qb[6], int qep[24],
+                      uint32_t& q0, uint32_t& q1) {
     float ep[24];
 #pragma unroll
     for (int i = 0; i < 24; i++) {
-        ep[i] = 0.0f;
+        ep[i] = i < 16 ? ep0[i] : 0.0f;
         qep[i] = 0;
     }
     uint32_t pattern = kPartitionMap[part_id];
-#pragma unroll
-    for (int j = 0; j < 2; j++) block_segment<3, false>(blk, subset_mask_from_map(pattern, j), ep + 8 * j);
     quant_dequant<2>(qep, ep, epb, qb);
     return block_quant<3, 3, 2>(blk, ep, pattern, q0, q1);
 }
 
 // The refinement of a two-region encode's winner (bc6h.rs:355-387): the
 // best endpoints (qep[0..16), channel 3 unused) and indices.
-BCN_DEV float refine_2p(const Blk& blk, int part_id, const Job& st, float best_err, uint32_t iters,
-                        int best_qep[16], uint32_t& bq0, uint32_t& bq1) {
+BCN_DEV float refine_2p(const Blk& blk, int part_id, const float ep0[16], const Job& st, float best_err,
+                        uint32_t iters, int best_qep[16], uint32_t& bq0, uint32_t& bq1) {
     int qe[24];
-    eval_2p(blk, part_id, st.epb, st.qb, qe, bq0, bq1);
+    eval_2p(blk, part_id, ep0, st.epb, st.qb, qe, bq0, bq1);
 #pragma unroll
     for (int i = 0; i < 16; i++) best_qep[i] = qe[i];
     uint32_t pattern = kPartitionMap[part_id];
@@ -515,6 +516,7 @@ struct Work {
     unsigned long long* keys;  // [j * npad + block], 2-region encodes: (error bits << 32) | candidate
     float* slot_err;           // [j * npad + block]
     uint4* slot_pay;           // [(j * 3 + r) * npad + block]: the encode's result, coded by select only if it wins
+    float4* seg;               // [(c * 4 + q) * npad + block]: list entry c's unquantised endpoints (16 floats)
     BC6HSettingsDev S;
 };
 
@@ -728,6 +730,10 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_ker
     for (int i = 0; i < 16; i++) ep0[i] = 0.0f;
 #pragma unroll
     for (int h = 0; h < 2; h++) block_segment<3, false>(blk, subset_mask_from_map(pattern, h), ep0 + 8 * h);
+    // kept for the refinement of whichever encode picks this entry
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        w.seg[((size_t)c * 4 + q) * w.npad + gi] = make_float4(ep0[4 * q], ep0[4 * q + 1], ep0[4 * q + 2], ep0[4 * q + 3]);
 #pragma unroll 1
     for (int j = 0; j < P.n2; j++) {
         if (!scratch_ok(w, j, P.n2, gi)) continue;
@@ -748,7 +754,9 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_SEARCH_MINB) bc6h_search_ker
 }
 
 // K3: the winner of two-region encode blockIdx.y, refined (bc6h.rs:355-387);
-// one warp per tile, a private staged tile per warp.
+// one warp per tile, a private staged tile per warp. The winner's
+// unquantised endpoints come from the search's scratch (`seg`) instead of a
+// second endpoint fit of the same pixels.
 __global__ void __launch_bounds__(NW * 32, BCN_BC6H_REFINE_MINB) bc6h_refine2_kernel(Work w, uint32_t ntiles) {
     __shared__ float px[NW][48][NB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -763,10 +771,20 @@ __global__ void __launch_bounds__(NW * 32, BCN_BC6H_REFINE_MINB) bc6h_refine2_ke
     const unsigned long long key = w.keys[(size_t)j * w.npad + gi];
     if (gi < w.nblocks && key != ~0ull && scratch_ok(w, (int)(key & 0xFFFFFFFFull), P.k, gi)) {
         const Job st = unpack_job(w.jobs[(size_t)j * w.npad + gi]);
-        const int part = w.lists[(size_t)(key & 0xFFFFFFFFull) * w.npad + gi] & 31;
+        const int c = (int)(key & 0xFFFFFFFFull);
+        const int part = w.lists[(size_t)c * w.npad + gi] & 31;
+        float ep0[16];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float4 v = w.seg[((size_t)c * 4 + q) * w.npad + gi];
+            ep0[4 * q] = v.x;
+            ep0[4 * q + 1] = v.y;
+            ep0[4 * q + 2] = v.z;
+            ep0[4 * q + 3] = v.w;
+        }
         int qep[16];
         uint32_t q0, q1;
-        err = refine_2p(Blk{&px[warp][0][lane]}, part, st, __uint_as_float((uint32_t)(key >> 32)),
+        err = refine_2p(Blk{&px[warp][0][lane]}, part, ep0, st, __uint_as_float((uint32_t)(key >> 32)),
                         w.S.refine_iterations_2p, qep, q0, q1);
         store_pay(w, j, gi, qep, q0, q1, part);
     }
@@ -838,7 +856,7 @@ __global__ void __launch_bounds__(128) bc6h_select_kernel(Work w, int n, int n2)
 
 // Scratch layout, each array 256-byte aligned.
 struct Layout {
-    size_t jobs, lists, keys, slot_err, slot_pay, total;
+    size_t jobs, lists, keys, slot_err, slot_pay, seg, total;
 };
 static Layout layout(uint32_t npad, const Plan& P) {
     auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
@@ -848,7 +866,8 @@ static Layout layout(uint32_t npad, const Plan& P) {
     L.keys = up(L.lists + (size_t)(P.k > 0 ? P.k : 1) * npad);
     L.slot_err = up(L.keys + (size_t)(P.n2 > 0 ? P.n2 : 1) * npad * sizeof(unsigned long long));
     L.slot_pay = up(L.slot_err + (size_t)P.n * npad * sizeof(float));
-    L.total = up(L.slot_pay + (size_t)P.n * 3 * npad * sizeof(uint4));
+    L.seg = up(L.slot_pay + (size_t)P.n * 3 * npad * sizeof(uint4));
+    L.total = up(L.seg + (size_t)(P.k > 0 ? P.k : 1) * 4 * npad * sizeof(float4));
     return L;
 }
 
@@ -921,6 +940,7 @@ cudaError_t launch_bc6h_encode(const void* src, size_t stride_bytes, int source_
     w.keys = (unsigned long long*)(base + L.keys);
     w.slot_err = (float*)(base + L.slot_err);
     w.slot_pay = (uint4*)(base + L.slot_pay);
+    w.seg = (float4*)(base + L.seg);
     w.S = settings;
     cudaError_t e;
     bc6h_prep_kernel<<<ntiles, NW * 32, 0, s>>>(w);
